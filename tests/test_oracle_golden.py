@@ -1,0 +1,134 @@
+"""Pin the CPU oracle against the reference's Julia golden vectors (n=7 RK4 steps).
+
+Tolerances: lensing and logpdf at rounding level.  Two documented gaps are
+excluded or bounded loosely because they sit between the reference's own
+code and the Julia goldens, not in the restatement:
+
+* adjoint lensing and gradf differ on the half-axis Nyquist column / the
+  N/2 row (the reference's EB<->QU Nyquist convention, util.py:143,155);
+* grad_phi: the reference integrates a continuous adjoint for delta-phi
+  (lense_flow.py:195-252) whose discretisation differs from Julia's; it
+  agrees with Julia exactly on the KY=0 column and to ~5e-4 elsewhere, and
+  with finite differences of its own logpdf to ~1e-5.
+"""
+import numpy as np
+import pytest
+
+from conftest import load_golden, rel_l2
+from oracle import lenseflow_ref as R
+
+N = 256
+NSTEPS = 7
+
+
+def _interior_mask(idx, nside=N):
+    """Entries off the half-axis DC/Nyquist columns and the N/2 row."""
+    r, c = idx
+    return (c != 0) & (c != nside // 2) & (r != nside // 2)
+
+
+def _lens_set(name):
+    g = load_golden(name)
+    phi = R.map_(R.FlatS0(scalar_matrix=g["phi"]))
+    return g, phi
+
+
+@pytest.mark.parametrize("adjoint", [False, True])
+def test_lens_T(adjoint):
+    g, phi = _lens_set("lens_I.npz")
+    t = R.map_(R.FlatS0(scalar_matrix=g["t"]))
+    out = R.fourier(R.lense_flow(t, phi, n=NSTEPS, adjoint=adjoint)).scalar_matrix
+    key = "t_adjoint" if adjoint else "t_lensed"
+    r, c = g["idx"]
+    m = _interior_mask(g["idx"]) if adjoint else np.ones(r.shape, bool)
+    assert rel_l2(out[r, c][m], g[key][m]) < 1e-11
+
+
+@pytest.mark.parametrize("adjoint", [False, True])
+def test_lens_QU(adjoint):
+    g, phi = _lens_set("lens_P.npz")
+    qu = R.map_(R.eb2qu(R.FlatS2(polar_matrix_1=g["e"], polar_matrix_2=g["b"])))
+    out = R.qu2eb(R.fourier(R.lense_flow(qu, phi, n=NSTEPS, adjoint=adjoint)))
+    pre = "adjoint" if adjoint else "lensed"
+    r, c = g["idx"]
+    m = _interior_mask(g["idx"]) if adjoint else np.ones(r.shape, bool)
+    assert rel_l2(out.polar_matrix_1[r, c][m], g["e_" + pre][m]) < 1e-11
+    assert rel_l2(out.polar_matrix_2[r, c][m], g["b_" + pre][m]) < 1e-11
+
+
+@pytest.mark.parametrize("adjoint", [False, True])
+def test_lens_TQU(adjoint):
+    g, phi = _lens_set("lens_IP.npz")
+    f = R.map_(R.eb2qu(R.FlatS02(scalar_matrix=g["t"], polar_matrix_1=g["e"], polar_matrix_2=g["b"])))
+    out = R.qu2eb(R.fourier(R.lense_flow(f, phi, n=NSTEPS, adjoint=adjoint)))
+    pre = "adjoint" if adjoint else "lensed"
+    r, c = g["idx"]
+    m = _interior_mask(g["idx"]) if adjoint else np.ones(r.shape, bool)
+    assert rel_l2(out.scalar_matrix[r, c][m], g["t_" + pre][m]) < 1e-11
+    assert rel_l2(out.polar_matrix_1[r, c][m], g["e_" + pre][m]) < 1e-11
+    assert rel_l2(out.polar_matrix_2[r, c][m], g["b_" + pre][m]) < 1e-11
+
+
+def test_inverse_round_trip_T():
+    """Inverse lensing is pinned by round trip, as in the reference (test_lensing.py:97-161)."""
+    g, phi = _lens_set("lens_I.npz")
+    t = R.map_(R.FlatS0(scalar_matrix=g["t"]))
+    lensed = R.lense_flow(t, phi, n=NSTEPS)
+    back = R.lense_flow(lensed, phi, n=NSTEPS, direction=R.INVERSE_LENSE)
+    assert rel_l2(back.scalar_matrix, t.scalar_matrix) < 1e-5
+
+
+def _infer_I():
+    gl = load_golden("lens_I.npz")
+    g = load_golden("infer_I.npz")
+    w = R.get_fourier_weights((N, N))
+    D = lambda m: R.DiagonalScalar(scalar_matrix=m, fourier_weights=w)
+    S = dict(field=R.FlatS0(scalar_matrix=gl["t"], fourier_weights=w),
+             phi=R.FlatS0(scalar_matrix=gl["phi"], fourier_weights=w),
+             data=R.FlatS0(scalar_matrix=g["data_t"], fourier_weights=w),
+             Cn=D(g["cn"]), Cphi=D(g["cphi"]), Cf=D(g["cf"]), M=D(g["m"]), B=D(g["b"]))
+    return g, S
+
+
+def _infer_P():
+    gl = load_golden("lens_P.npz")
+    g = load_golden("infer_P.npz")
+    w = R.get_fourier_weights((N, N))
+    D = lambda p: R.DiagonalEB(matrix_EE=g[p + "_ee"], matrix_BB=g[p + "_bb"], fourier_weights=w)
+    S = dict(field=R.FlatS2(polar_matrix_1=gl["e"], polar_matrix_2=gl["b"], fourier_weights=w),
+             phi=R.FlatS0(scalar_matrix=gl["phi"], fourier_weights=w),
+             data=R.FlatS2(polar_matrix_1=g["data_e"], polar_matrix_2=g["data_b"], fourier_weights=w),
+             Cn=D("cn"), Cphi=R.DiagonalScalar(scalar_matrix=g["cphi"], fourier_weights=w), Cf=D("cf"),
+             M=D("m"), B=D("b"))
+    return g, S
+
+
+@pytest.mark.parametrize("which", ["I", "P"])
+def test_logpdf(which):
+    """The Julia value uses DC/Nyquist weight 1 (util.py:90-96), not the 0.5 default of constants.py:21."""
+    g, S = _infer_I() if which == "I" else _infer_P()
+    v = R.logpdf(S["field"], S["phi"], S["data"], S["Cn"], S["Cphi"], S["Cf"], S["M"], S["B"], n=NSTEPS)
+    assert abs(v - float(g["logpdf"])) / abs(float(g["logpdf"])) < 1e-12
+
+
+@pytest.mark.parametrize("which", ["I", "P"])
+def test_gradf(which):
+    g, S = _infer_I() if which == "I" else _infer_P()
+    out = R.gradf_logpdf(S["field"], S["phi"], S["data"], S["Cf"], S["Cn"], S["M"], S["B"], n=NSTEPS)
+    r, c = g["idx"]
+    m = _interior_mask(g["idx"])
+    if which == "I":
+        pairs = [(out.scalar_matrix, g["gradf"])]
+    else:
+        pairs = [(out.polar_matrix_1, g["gradf_e"]), (out.polar_matrix_2, g["gradf_b"])]
+    for a, gold in pairs:
+        assert rel_l2(a[r, c][m], gold[m]) < 1e-10
+
+
+def test_grad_phi_T():
+    g, S = _infer_I()
+    out = R.grad_phi_logpdf(S["field"], S["phi"], S["data"], S["Cn"], S["Cphi"], S["Cf"], S["M"], S["B"], n=NSTEPS)
+    r, c = g["idx"]
+    ky0 = (c == 0) & (r != N // 2)
+    assert rel_l2(out[r, c][ky0], g["grad_phi"][ky0]) < 1e-9
+    assert rel_l2(out[r, c], g["grad_phi"]) < 1e-3
