@@ -1,0 +1,407 @@
+#!/usr/bin/env python
+"""LenseFlow throughput benchmark: 512^2 QU maps/s on B200 (one JSON line on rank 0).
+
+Workload (one "step"): a batch of B = 64 independent (QU field, phi) pairs,
+512 x 512, 2 arcmin pixels, forward LenseFlow with 7 RK4 steps in FP32,
+including the float64 phi-derivative precompute (a new phi per map).
+Inputs are seeded Gaussian random fields (8 distinct maps tiled to the batch)
+with the workload's spectra; the batch's working set (~1.4 GB) is far larger
+than the 126 MB L2, so no flush is needed between steps.
+
+``value``  : maps/s with inputs resident in HBM, CUDA events on the launching
+             stream, max over ranks.
+``e2e``    : the same metric through the public host-buffer API
+             (engine.HostPipeline): float64 fields and phi copied from pinned
+             host memory, derivative precompute with the magnification check,
+             lens, float64 result copied back, every step.
+``roofline``: the dominant kernel's algorithmic bytes per launch over its
+             average event-timed duration inside the timed region.
+Multi-GPU: every rank lenses its own batch (no collective; weak scaling).
+``--impl reference`` times the float64 CPU oracle on the host cores instead.
+"""
+import argparse
+import json
+import math
+import os
+import subprocess
+import sys
+import threading
+import time
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+METRIC = "LenseFlow 512x512 QU maps/s (FP32, nsteps=7, incl. phi precompute)"
+UNIT = "maps/s"
+
+
+def parse():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=10)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--batch", type=int, default=64)
+    ap.add_argument("--nside", type=int, default=512)
+    ap.add_argument("--ncomp", type=int, default=2)
+    ap.add_argument("--nsteps", type=int, default=7)
+    ap.add_argument("--theta", type=float, default=2.0)
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-fp64", action="store_true")
+    ap.add_argument("--no-e2e", action="store_true")
+    return ap.parse_args()
+
+
+def workload_config(a):
+    return {"workload": f"lenseflow_fwd_qu{a.nside}_b{a.batch}_n{a.nsteps}" if a.ncomp == 2 else
+            f"lenseflow_fwd_c{a.ncomp}_{a.nside}_b{a.batch}_n{a.nsteps}",
+            "nside": a.nside, "ncomp": a.ncomp, "batch_per_gpu": a.batch, "rk4_steps": a.nsteps,
+            "theta_pix_arcmin": a.theta,
+            "phi_spectrum": "1/[l^2 (l+1)^2 (1+(l/60)^2)], 2.5' rms deflection (well-posed reading)",
+            "fields": "QU from E ~ l^-2 exp(-(l/2000)^2), 5 uK rms, B=0" if a.ncomp == 2 else "T",
+            "l2": "inputs larger than L2 (working set ~1.4 GB per GPU), no flush",
+            "parallelism": f"replicas x{a.gpus} (independent batches, no collective)"}
+
+
+# ------------------------------------------------------------------ CPU legs
+def _cpu_lens_one(args):
+    """One map through the float64 oracle (runs in a spawned worker)."""
+    os.environ.setdefault("OMP_NUM_THREADS", "1")
+    sys.path.insert(0, ROOT)
+    from oracle import lenseflow_ref as R
+    from cmblensing_b200.simulate import lens_batch
+    N, theta, C, n, seed = args
+    f, phis = lens_batch(N, theta, 1, C, seed0=seed)
+    pw = R.pix_width_of(theta)
+    d = R.phi_derivatives(phis[0], pw)
+    t0 = time.perf_counter()
+    for c in range(C):
+        R.primal_lense_flow(f[0, c], phis[0], pw, n, 1, False, d)
+    return time.perf_counter() - t0
+
+
+class CpuPool:
+    """Spawned process pool, one single-threaded worker per host core."""
+
+    def __init__(self):
+        import multiprocessing as mp
+        self.cores = os.cpu_count() or 1
+        self.pool = mp.get_context("spawn").Pool(self.cores, initializer=_set_single_thread)
+
+    def run(self, a, nmaps, seed=0):
+        """(time, CPU seconds) to lens ``nmaps`` maps, one per worker in parallel.
+
+        The time is the slowest worker's lens time: input generation, done in
+        the workers before their clocks start, is excluded.
+        """
+        jobs = [(a.nside, a.theta, a.ncomp, a.nsteps, seed + i) for i in range(nmaps)]
+        per = self.pool.map(_cpu_lens_one, jobs, chunksize=1)
+        waves = math.ceil(nmaps / self.cores)
+        return max(per) * waves, sum(per)
+
+    def close(self):
+        self.pool.close()
+        self.pool.join()
+
+
+def _set_single_thread():
+    for v in ("OMP_NUM_THREADS", "OPENBLAS_NUM_THREADS", "MKL_NUM_THREADS"):
+        os.environ[v] = "1"
+
+
+def cpu_describe():
+    try:
+        for line in open("/proc/cpuinfo"):
+            if line.startswith("model name"):
+                return line.split(":", 1)[1].strip()
+    except OSError:
+        pass
+    return "unknown"
+
+
+def run_reference(a):
+    rank = int(os.environ.get("RANK", "0"))
+    if rank != 0:
+        return
+    pool = CpuPool()
+    nmaps = pool.cores
+    for i in range(max(a.warmup, 0)):
+        pool.run(a, nmaps, seed=100 * i)
+    walls = []
+    for i in range(a.steps):
+        w, _ = pool.run(a, nmaps, seed=1000 + 100 * i)
+        walls.append(w)
+    pool.close()
+    total = sum(walls)
+    value = nmaps * a.steps / total
+    sample = (f"{nmaps} maps per step ({a.nside}^2, C={a.ncomp}, n={a.nsteps}, float64 numpy oracle, "
+              f"one map per process), {pool.cores} processes on {cpu_describe()}")
+    line = {"impl": "reference", "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": a.gpus,
+            "steps": a.steps, "warmup": a.warmup, "ms_per_step": 1000 * total / a.steps, "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+            "config": workload_config(a),
+            "cpu_baseline": {"value": value, "unit": UNIT, "cores": pool.cores, "kind": "port", "sample": sample},
+            "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+            "note": "reference = float64 numpy restatement of cmb_lensing/lense_flow.py (jax is not installed)"}
+    print(json.dumps(line), flush=True)
+
+
+# ------------------------------------------------------------------- clocks
+class ClockSampler:
+    FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, index):
+        self.index = index
+        self.rows = []
+        self.proc = None
+
+    def start(self):
+        try:
+            self.proc = subprocess.Popen(["nvidia-smi", "-i", str(self.index), f"--query-gpu={self.FIELDS}",
+                                          "--format=csv,noheader,nounits", "-lms", "200"],
+                                         stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+            self.thread = threading.Thread(target=self._read, daemon=True)
+            self.thread.start()
+        except OSError:
+            self.proc = None
+
+    def _read(self):
+        for line in self.proc.stdout:
+            self.rows.append([x.strip() for x in line.split(",")])
+
+    def stop(self):
+        if self.proc is None:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
+        self.proc.terminate()
+        try:
+            self.proc.wait(timeout=5)
+        except subprocess.TimeoutExpired:
+            self.proc.kill()
+        sm, mx, reasons = [], None, set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for r in self.rows:
+            try:
+                sm.append(float(r[1]))
+                mx = float(r[2])
+                for nm, v in zip(names, r[5:9]):
+                    if v.strip().lower() == "active":
+                        reasons.add(nm)
+            except (ValueError, IndexError):
+                continue
+        sm.sort()
+        med = sm[len(sm) // 2] if sm else None
+        return {"sm_mhz": med, "sm_max_mhz": mx, "reasons": sorted(reasons), "samples": len(sm)}
+
+
+# ----------------------------------------------------------- algorithmic bytes
+def row_bytes_per_lens(C, n, P, in_bytes=4, out_bytes=4):
+    """Bytes the row kernels of one forward lens must move per map (float32 state, 5 phi planes).
+
+    init: read f, write y0 and S.  Stage 1: read Gx, S, y0, phi(5); write acc, S.
+    Stages 2-3: also read acc.  Stage 4: read Gx, S, y0, acc, phi; write y0 and S
+    (the last stage writes the output instead and no S).
+    """
+    init = (in_bytes + 8) * C
+    s1 = 20 * C + 20
+    s23 = 24 * C + 20
+    s4 = 24 * C + 20
+    last_adj = -8 * C + out_bytes * C  # last stage: no y0/S writes, one output write
+    total = init + n * (s1 + 2 * s23 + s4) + last_adj
+    return total * P
+
+
+def col_bytes_per_lens(C, n, P):
+    """Column kernels: read and write one row-spectral array (N x N/2 complex64 = 4P bytes) per plane."""
+    return 4 * n * 8 * C * P
+
+
+def survey_bytes_per_map(C, n, P):
+    """Minimal-pass model: 4n(36C+20)P + 8CP + 140P (phi precompute)."""
+    return (4 * n * (36 * C + 20) + 8 * C + 140) * P
+
+
+# --------------------------------------------------------------------- main
+def main():
+    a = parse()
+    if a.impl == "reference":
+        run_reference(a)
+        return
+    rank = int(os.environ.get("RANK", "0"))
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    pool = None
+    if rank == 0 and world == 1 and not a.no_cpu_baseline:
+        pool = CpuPool()  # spawn before any CUDA work
+
+    import numpy as np
+    import torch
+    torch.cuda.set_device(local)
+    dev = torch.device("cuda", local)
+    dist = None
+    if world > 1:
+        import datetime
+        import torch.distributed as dist
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=300))
+
+    from cmblensing_b200 import _native as nat
+    from cmblensing_b200 import engine
+    from cmblensing_b200.simulate import lens_batch, ARCMIN
+
+    N, C, B, n = a.nside, a.ncomp, a.batch, a.nsteps
+    P = N * N
+    pw = a.theta * ARCMIN
+    uniq = min(8, B)
+    f_u, phi_u = lens_batch(N, a.theta, uniq, C, seed0=17 * rank)
+    reps = [i % uniq for i in range(B)]
+    f_host = np.ascontiguousarray(f_u[reps])
+    phi_host = np.ascontiguousarray(phi_u[reps])
+
+    plan = engine.get_plan(N, C, pw, "f32", device=dev)
+    f_dev = torch.as_tensor(f_host, device=dev, dtype=torch.float32)
+    phi_dev = torch.as_tensor(phi_host, device=dev)
+    out_dev = torch.empty_like(f_dev)
+    planes = torch.empty((B, 5, N, N), dtype=torch.float32, device=dev)
+    ws = torch.empty(plan.workspace_bytes(B, False), dtype=torch.uint8, device=dev)
+    phi_ws = torch.empty(plan.phi_workspace_bytes(B), dtype=torch.uint8, device=dev)
+
+    def step():
+        plan.phi_planes(phi_dev, check_det=False, out=planes, workspace=phi_ws)
+        plan.lense_flow(f_dev, planes, n=n, out=out_dev, workspace=ws)
+
+    # the magnification check once, outside the timed region
+    plan.phi_planes(phi_dev[:uniq], check_det=True)
+    for _ in range(a.warmup):
+        step()
+    torch.cuda.synchronize()
+
+    def barrier():
+        if dist is not None:
+            dist.barrier()
+        torch.cuda.synchronize()
+
+    clocks = ClockSampler(local)
+    clocks.start()
+    plan.profile_reset()
+    plan.profile(True)
+    barrier()
+    ev0 = torch.cuda.Event(enable_timing=True)
+    ev1 = torch.cuda.Event(enable_timing=True)
+    ev0.record()
+    for _ in range(a.steps):
+        step()
+    ev1.record()
+    barrier()
+    plan.profile(False)
+    ms = ev0.elapsed_time(ev1)
+    clk = clocks.stop()
+    row_ms, row_n = plan.profile_read(nat.LF_KIND_ROW)
+    col_ms, col_n = plan.profile_read(nat.LF_KIND_COL)
+    phi_ms, phi_n = plan.profile_read(nat.LF_KIND_PHI)
+    if dist is not None:
+        t = torch.tensor([ms], device=dev)
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        ms = float(t.item())
+    value = world * B * a.steps / (ms / 1000.0)
+
+    # parity spot check of this run's output (one map) against the first lens of the batch in FP64 engine
+    peaks = {}
+    try:
+        peaks = json.load(open(os.path.join(ROOT, "MEASURED_PEAKS.json")))
+    except (OSError, ValueError):
+        pass
+    hbm_peak = float(peaks.get("hbm_gbs", 6650.0))
+    peak_src = "measured" if "hbm_gbs" in peaks else "fallback"
+
+    row_b = row_bytes_per_lens(C, n, P, 4, 4) * B / max(4 * n + 1, 1)  # per launch, all maps
+    col_b = col_bytes_per_lens(C, n, P) * B / max(4 * n, 1)
+    kinds = {"row": (row_ms, row_n, row_b), "col": (col_ms, col_n, col_b)}
+    dom = max(kinds, key=lambda k: kinds[k][0])
+    k_ms, k_n, k_b = kinds[dom]
+    avg_s = (k_ms / max(k_n, 1)) / 1000.0
+    achieved = k_b / avg_s / 1e9 if avg_s > 0 else 0.0
+    step_gbs = survey_bytes_per_map(C, n, P) * (value / world) / 1e9
+
+    result = {"metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": a.steps,
+              "warmup": a.warmup, "ms_per_step": ms / a.steps, "higher_is_better": True, "scaling": "weak",
+              "vs_baseline": None, "dtype": "f32", "data": "synthetic", "config": workload_config(a),
+              "roofline": {"bound": "hbm", "kernel": f"k_row (RK4 row pass + fused epilogue)" if dom == "row"
+                           else "k_col (column FFT pass)", "achieved": achieved, "peak": hbm_peak,
+                           "unit": "GB/s", "frac": achieved / hbm_peak, "traffic": None,
+                           "peak_source": peak_src,
+                           "bytes_per_launch": k_b, "avg_launch_ms": avg_s * 1000.0,
+                           "step_model_gbs": step_gbs, "step_model_frac": step_gbs / hbm_peak,
+                           "step_model": "(4n(36C+20)+8C+140) N^2 bytes per map"},
+              "kernel_ms_per_step": {"row": row_ms / a.steps, "col": col_ms / a.steps, "phi": phi_ms / a.steps},
+              "gpu_launches": (row_n + col_n + phi_n) // a.steps * a.steps,
+              "clocks": clk}
+
+    # ------------------------------------------------------------ e2e leg
+    if not a.no_e2e:
+        pipe = engine.HostPipeline(plan, B, io_dtype=torch.float64)
+        fh = torch.from_numpy(f_host).pin_memory()
+        ph = torch.from_numpy(phi_host).pin_memory()
+        oh = torch.empty_like(fh).pin_memory()
+        for _ in range(max(a.warmup, 1)):
+            pipe(fh, ph, oh, n=n)
+        torch.cuda.synchronize()
+        barrier()
+        e0 = torch.cuda.Event(enable_timing=True)
+        e1 = torch.cuda.Event(enable_timing=True)
+        e0.record()
+        for _ in range(a.steps):
+            pipe(fh, ph, oh, n=n)
+        e1.record()
+        barrier()
+        ems = e0.elapsed_time(e1)
+        if dist is not None:
+            t = torch.tensor([ems], device=dev)
+            dist.all_reduce(t, op=dist.ReduceOp.MAX)
+            ems = float(t.item())
+        result["e2e"] = {"value": world * B * a.steps / (ems / 1000.0), "unit": UNIT,
+                         "h2d_bytes_per_step": pipe.h2d_bytes(), "d2h_bytes_per_step": pipe.d2h_bytes(),
+                         "api": "engine.HostPipeline (float64 host I/O, pinned)"}
+        # parity of the bench output against the device-resident leg
+        diff = float((torch.as_tensor(oh[:1], device=dev).float() - out_dev[:1]).norm() / out_dev[:1].norm())
+        result["e2e"]["rel_l2_vs_device_leg"] = diff
+
+    # ---------------------------------------------------- FP64 comparator
+    if not a.no_fp64 and rank == 0:
+        sys.path.insert(0, os.path.join(ROOT, "baseline"))
+        from fp64_torch import lense_flow_fp64
+        nb = 4
+        f64 = torch.as_tensor(f_host[:nb], device=dev)
+        p64 = torch.as_tensor(phi_host[:nb], device=dev)
+        lense_flow_fp64(f64, p64, pw, n)
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        ref64 = lense_flow_fp64(f64, p64, pw, n)
+        torch.cuda.synchronize()
+        dt = time.perf_counter() - t0
+        ours = out_dev[:nb].double()
+        rel = float((ours - ref64).norm() / ref64.norm())
+        result["fp64_restatement"] = {"value": nb / dt, "unit": UNIT, "batch": nb,
+                                      "what": "torch float64 restatement of the reference op sequence (cuFFT), "
+                                              "not the reference", "speedup_of_value": value / world / (nb / dt),
+                                      "rel_l2_fp32_vs_fp64": rel}
+
+    # ---------------------------------------------------- CPU baseline
+    if pool is not None:
+        nm = pool.cores
+        pool.run(a, min(nm, 2))  # warm the workers (imports)
+        wall, busy = pool.run(a, nm, seed=500)
+        pool.close()
+        result["cpu_baseline"] = {"value": nm / wall, "unit": UNIT, "cores": pool.cores, "kind": "port",
+                                  "sample": f"{nm} maps ({N}^2, C={C}, n={n}) through the float64 numpy oracle, "
+                                            f"one single-threaded process per core on {cpu_describe()}; "
+                                            f"{busy:.1f} s of CPU work"}
+    if rank == 0:
+        print(json.dumps(result), flush=True)
+    if dist is not None:
+        dist.barrier()
+        dist.destroy_process_group()
+
+
+if __name__ == "__main__":
+    main()

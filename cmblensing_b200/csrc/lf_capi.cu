@@ -1,0 +1,412 @@
+// C ABI of the LenseFlow engine: plans, launch sequencing, validation.
+#include <cuda_runtime.h>
+#include <stdint.h>
+
+#include <cmath>
+#include <cstring>
+#include <new>
+#include <vector>
+
+#include "../../include/lenseflow.h"
+#include "lf_kernels.cuh"
+
+using namespace lf;
+
+// Launch timing: when enabled, an event pair brackets every launch on the
+// launching stream, tagged with the kernel kind (LF_KIND_*).
+struct Prof {
+  bool on = false;
+  std::vector<cudaEvent_t> pool;
+  size_t used = 0;
+  std::vector<int> kind;  // one per recorded launch
+  cudaEvent_t next() {
+    if (used == pool.size()) {
+      cudaEvent_t e;
+      if (cudaEventCreate(&e) != cudaSuccess) return nullptr;
+      pool.push_back(e);
+    }
+    return pool[used++];
+  }
+};
+
+struct lf_plan_s {
+  Prof prof;
+  int N;
+  int C;
+  int prec;
+  double pix_width;
+  int device;
+  void* tw;        // N complex values in the compute precision
+  double2* tw64;   // N complex float64 (phi precompute)
+};
+
+namespace {
+
+constexpr int kVersion = 100;
+
+bool valid_n(int n) { return n == 64 || n == 128 || n == 256 || n == 512 || n == 1024; }
+
+int cuda_status(cudaError_t e) {
+  if (e == cudaSuccess) return LF_OK;
+  if (e == cudaErrorMemoryAllocation) return LF_ERR_OOM;
+  return LF_ERR_CUDA;
+}
+
+// Launch geometry per (precision, N).
+template <typename T> struct Geo;
+template <> struct Geo<float> {
+  static constexpr int LINES = 16;
+  static constexpr int nt(int n) { return n <= 64 ? 128 : (n <= 512 ? 256 : 512); }
+};
+template <> struct Geo<double> {
+  static constexpr int LINES = 8;
+  static constexpr int nt(int n) { return n <= 64 ? 64 : (n <= 128 ? 128 : (n <= 512 ? 256 : 512)); }
+};
+
+// Opt in to > 48 KB of dynamic shared memory once per kernel and device.
+template <auto Kernel>
+cudaError_t ensure_smem(size_t smem) {
+  static size_t done[64] = {0};
+  int dev = 0;
+  cudaGetDevice(&dev);
+  if (dev < 0 || dev >= 64) return cudaErrorInvalidDevice;
+  if (done[dev] >= smem) return cudaSuccess;
+  cudaError_t e = cudaFuncSetAttribute(Kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+  if (e == cudaSuccess) done[dev] = smem;
+  return e;
+}
+
+thread_local Prof* g_prof = nullptr;  // profiler of the plan whose call is running on this thread
+
+template <auto Kernel, typename... Args>
+cudaError_t launch_k(int kind, dim3 grid, int nt, size_t smem, cudaStream_t st, Args... args) {
+  cudaError_t e = ensure_smem<Kernel>(smem);
+  if (e != cudaSuccess) return e;
+  Prof* pf = (g_prof && g_prof->on) ? g_prof : nullptr;
+  cudaEvent_t e0 = pf ? pf->next() : nullptr, e1 = pf ? pf->next() : nullptr;
+  if (e0) cudaEventRecord(e0, st);
+  Kernel<<<grid, nt, smem, st>>>(args...);
+  e = cudaGetLastError();
+  if (e1) {
+    cudaEventRecord(e1, st);
+    pf->kind.push_back(kind);
+  }
+  return e;
+}
+
+template <auto Kernel, typename... Args>
+cudaError_t launch(dim3 grid, int nt, size_t smem, cudaStream_t st, Args... args) {
+  return launch_k<Kernel>(LF_KIND_PHI, grid, nt, smem, st, args...);
+}
+
+template <typename T, int N, int C, bool ADJ>
+cudaError_t run_lens_n(const StageArgs& base, int B, int nsteps, double t0, double t1, cudaStream_t st) {
+  constexpr int LINES = Geo<T>::LINES;
+  constexpr int NT = Geo<T>::nt(N);
+  constexpr int H = N / 2;
+  const size_t smem_row = sizeof(c2<T>) * (N + 2 * LINES * H);
+  const size_t smem_col = sizeof(c2<T>) * (N + LINES * N);
+  const dim3 grow(N / LINES, B);
+  const dim3 gcol(H / LINES, B * C);
+  StageArgs a = base;
+  cudaError_t e;
+  const double h = (t1 - t0) / nsteps;  // util.py:185
+  const double hh = h / 2.0;
+  a.h = h;
+  a.stage = 0;
+  a.last = 0;
+  a.t_cur = t0;
+  a.t_next = t0;
+  e = launch_k<k_row<T, N, C, ADJ, true, LINES, NT>>(LF_KIND_ROW, grow, NT, smem_row, st, a);
+  if (e != cudaSuccess) return e;
+  for (int i = 0; i < nsteps; ++i) {
+    const double t = t0 + i * h;  // util.py:189
+    const double tc[4] = {t, t + hh, t + hh, t + h};
+    const double tn[4] = {t + hh, t + hh, t + h, t0 + (i + 1) * h};
+    for (int s = 0; s < 4; ++s) {
+      a.stage = s + 1;
+      a.t_cur = tc[s];
+      a.t_next = tn[s];
+      a.last = (i == nsteps - 1 && s == 3);
+      e = launch_k<k_col<T, N, LINES, NT>>(LF_KIND_COL, gcol, NT, smem_col, st, a);
+      if (e != cudaSuccess) return e;
+      e = launch_k<k_row<T, N, C, ADJ, false, LINES, NT>>(LF_KIND_ROW, grow, NT, smem_row, st, a);
+      if (e != cudaSuccess) return e;
+    }
+  }
+  return cudaSuccess;
+}
+
+template <typename T, int N>
+cudaError_t run_lens_c(int C, bool adj, const StageArgs& a, int B, int nsteps, double t0, double t1,
+                       cudaStream_t st) {
+  if (C == 1) return adj ? run_lens_n<T, N, 1, true>(a, B, nsteps, t0, t1, st) : run_lens_n<T, N, 1, false>(a, B, nsteps, t0, t1, st);
+  if (C == 2) return adj ? run_lens_n<T, N, 2, true>(a, B, nsteps, t0, t1, st) : run_lens_n<T, N, 2, false>(a, B, nsteps, t0, t1, st);
+  return adj ? run_lens_n<T, N, 3, true>(a, B, nsteps, t0, t1, st) : run_lens_n<T, N, 3, false>(a, B, nsteps, t0, t1, st);
+}
+
+template <typename T>
+cudaError_t run_lens(int N, int C, bool adj, const StageArgs& a, int B, int nsteps, double t0, double t1,
+                     cudaStream_t st) {
+  switch (N) {
+    case 64: return run_lens_c<T, 64>(C, adj, a, B, nsteps, t0, t1, st);
+    case 128: return run_lens_c<T, 128>(C, adj, a, B, nsteps, t0, t1, st);
+    case 256: return run_lens_c<T, 256>(C, adj, a, B, nsteps, t0, t1, st);
+    case 512: return run_lens_c<T, 512>(C, adj, a, B, nsteps, t0, t1, st);
+    default: return run_lens_c<T, 1024>(C, adj, a, B, nsteps, t0, t1, st);
+  }
+}
+
+template <typename TO, int N>
+cudaError_t run_phi_n(const void* phi, int basis, int B, TO* planes, int* min_det, void* ws, const double2* tw64,
+                      double kbase, cudaStream_t st) {
+  constexpr int LINES = 8;
+  constexpr int NT = Geo<double>::nt(N);
+  constexpr int H = N / 2;
+  double2* spec = reinterpret_cast<double2*>(ws);            // [B][N][H+1]
+  double2* packed = spec + (size_t)B * N * (H + 1);          // [B][5][N][H]
+  const size_t smem_row = sizeof(double2) * (N + LINES * H);
+  const size_t smem_col = sizeof(double2) * (N + LINES * N);
+  const int ctiles = (H + 1 + LINES - 1) / LINES;
+  cudaError_t e;
+  if (basis == LF_PHI_MAP) {
+    e = launch<k_phi_rows_r2c<N, LINES, NT>>(dim3(N / LINES, B), NT, smem_row, st,
+                                             reinterpret_cast<const double*>(phi), spec, tw64);
+    if (e != cudaSuccess) return e;
+    e = launch<k_phi_cols_fwd<N, LINES, NT>>(dim3(ctiles, B), NT, smem_col, st, spec, tw64);
+    if (e != cudaSuccess) return e;
+  } else {
+    e = cudaMemcpyAsync(spec, phi, sizeof(double2) * (size_t)B * N * (H + 1), cudaMemcpyDeviceToDevice, st);
+    if (e != cudaSuccess) return e;
+  }
+  e = launch<k_phi_cols_deriv<N, LINES, NT>>(dim3(ctiles, B), NT, smem_col, st, (const double2*)spec, packed,
+                                             (const double2*)tw64, kbase);
+  if (e != cudaSuccess) return e;
+  e = launch<k_phi_rows_c2r<TO, N, LINES, NT>>(dim3(N / LINES, B * 5), NT, smem_row, st, (const double2*)packed,
+                                               planes, (const double2*)tw64);
+  if (e != cudaSuccess) return e;
+  if (min_det) {
+    const long P = (long)N * N;
+    e = launch<k_min_det<TO>>(dim3(32, B), 256, 0, st, (const TO*)planes, P, min_det);
+  }
+  return e;
+}
+
+template <typename TO>
+cudaError_t run_phi(int N, const void* phi, int basis, int B, TO* planes, int* min_det, void* ws, const double2* tw64,
+                    double kbase, cudaStream_t st) {
+  switch (N) {
+    case 64: return run_phi_n<TO, 64>(phi, basis, B, planes, min_det, ws, tw64, kbase, st);
+    case 128: return run_phi_n<TO, 128>(phi, basis, B, planes, min_det, ws, tw64, kbase, st);
+    case 256: return run_phi_n<TO, 256>(phi, basis, B, planes, min_det, ws, tw64, kbase, st);
+    case 512: return run_phi_n<TO, 512>(phi, basis, B, planes, min_det, ws, tw64, kbase, st);
+    default: return run_phi_n<TO, 1024>(phi, basis, B, planes, min_det, ws, tw64, kbase, st);
+  }
+}
+
+bool aligned16(const void* p) { return (reinterpret_cast<uintptr_t>(p) & 15u) == 0; }
+
+}  // namespace
+
+extern "C" {
+
+int lf_version(void) { return kVersion; }
+
+const char* lf_status_string(int s) {
+  switch (s) {
+    case LF_OK: return "ok";
+    case LF_ERR_BAD_SHAPE: return "bad shape (N must be 64, 128, 256, 512 or 1024; ncomp 1..3; batch >= 0)";
+    case LF_ERR_BAD_DTYPE: return "bad dtype";
+    case LF_ERR_BAD_ARG: return "bad argument (null or misaligned pointer, bad direction or step count)";
+    case LF_ERR_SINGULAR_MAGNIFICATION: return "det(I + t grad grad phi) <= 0 for some pixel and t in [0,1]";
+    case LF_ERR_OOM: return "out of device memory";
+    case LF_ERR_TIMEOUT: return "timeout";
+    case LF_ERR_CUDA: return "CUDA error";
+    case LF_ERR_WORKSPACE: return "workspace too small";
+    default: return "unknown status";
+  }
+}
+
+int lf_plan_create(lf_plan_t* out, int nside, int ncomp, double pix_width, int precision) {
+  if (!out) return LF_ERR_BAD_ARG;
+  *out = nullptr;
+  if (!valid_n(nside) || ncomp < 1 || ncomp > 3) return LF_ERR_BAD_SHAPE;
+  if (precision != LF_F32 && precision != LF_F64) return LF_ERR_BAD_DTYPE;
+  if (!(pix_width > 0.0) || !std::isfinite(pix_width)) return LF_ERR_BAD_ARG;
+  lf_plan_s* p = new (std::nothrow) lf_plan_s();
+  if (!p) return LF_ERR_OOM;
+  p->N = nside;
+  p->C = ncomp;
+  p->prec = precision;
+  p->pix_width = pix_width;
+  cudaGetDevice(&p->device);
+  // exp(-2 pi i k / N) in float64 on the host, rounded once to the compute precision
+  std::vector<double2> t64(nside);
+  std::vector<float2> t32(nside);
+  for (int k = 0; k < nside; ++k) {
+    const double ang = -2.0 * M_PI * (double)k / (double)nside;
+    t64[k] = make_double2(std::cos(ang), std::sin(ang));
+    t32[k] = make_float2((float)t64[k].x, (float)t64[k].y);
+  }
+  cudaError_t e = cudaMalloc(&p->tw64, sizeof(double2) * nside);
+  if (e == cudaSuccess) e = cudaMemcpy(p->tw64, t64.data(), sizeof(double2) * nside, cudaMemcpyHostToDevice);
+  if (e == cudaSuccess) {
+    if (precision == LF_F64) {
+      p->tw = p->tw64;
+    } else {
+      e = cudaMalloc(&p->tw, sizeof(float2) * nside);
+      if (e == cudaSuccess) e = cudaMemcpy(p->tw, t32.data(), sizeof(float2) * nside, cudaMemcpyHostToDevice);
+    }
+  }
+  if (e != cudaSuccess) {
+    lf_plan_destroy(p);
+    return cuda_status(e);
+  }
+  *out = p;
+  return LF_OK;
+}
+
+int lf_plan_destroy(lf_plan_t p) {
+  if (!p) return LF_OK;
+  if (p->tw && p->tw != p->tw64) cudaFree(p->tw);
+  if (p->tw64) cudaFree(p->tw64);
+  for (cudaEvent_t e : p->prof.pool) cudaEventDestroy(e);
+  delete p;
+  return LF_OK;
+}
+
+size_t lf_workspace_bytes(lf_plan_t p, int batch, int adjoint) {
+  if (!p || batch < 0) return 0;
+  const size_t el = p->prec == LF_F64 ? 8 : 4;
+  return el * (size_t)p->N * p->N * (size_t)batch * p->C * (adjoint ? 5 : 4);
+}
+
+size_t lf_phi_planes_bytes(lf_plan_t p, int batch) {
+  if (!p || batch < 0) return 0;
+  const size_t el = p->prec == LF_F64 ? 8 : 4;
+  return el * 5 * (size_t)p->N * p->N * (size_t)batch;
+}
+
+size_t lf_phi_workspace_bytes(lf_plan_t p, int batch) {
+  if (!p || batch < 0) return 0;
+  const size_t N = p->N, H = N / 2;
+  return sizeof(double2) * (size_t)batch * (N * (H + 1) + 5 * N * H);
+}
+
+int lf_min_det_init(int* min_det, int batch, void* stream) {
+  if (batch <= 0) return LF_OK;
+  if (!min_det) return LF_ERR_BAD_ARG;
+  return cuda_status(cudaMemsetAsync(min_det, 0x7f, sizeof(int) * (size_t)batch, (cudaStream_t)stream));
+}
+
+float lf_decode_min_det(int i) {
+  const int b = i >= 0 ? i : (i ^ 0x7fffffff);
+  float f;
+  std::memcpy(&f, &b, sizeof(f));
+  return f;
+}
+
+int lf_phi_precompute(lf_plan_t p, const void* phi, int basis, int batch, void* planes, int* min_det, void* ws,
+                      size_t ws_bytes, void* stream) {
+  if (!p) return LF_ERR_BAD_ARG;
+  if (batch < 0) return LF_ERR_BAD_SHAPE;
+  if (batch == 0) return LF_OK;
+  if (basis != LF_PHI_MAP && basis != LF_PHI_FOURIER) return LF_ERR_BAD_ARG;
+  if (!phi || !planes || !ws || !aligned16(phi) || !aligned16(planes) || !aligned16(ws)) return LF_ERR_BAD_ARG;
+  if (ws_bytes < lf_phi_workspace_bytes(p, batch)) return LF_ERR_WORKSPACE;
+  const double kbase = 2.0 * M_PI / ((double)p->N * p->pix_width);
+  cudaStream_t st = (cudaStream_t)stream;
+  cudaError_t e;
+  g_prof = &p->prof;
+  if (p->prec == LF_F64)
+    e = run_phi<double>(p->N, phi, basis, batch, reinterpret_cast<double*>(planes), min_det, ws, p->tw64, kbase, st);
+  else
+    e = run_phi<float>(p->N, phi, basis, batch, reinterpret_cast<float*>(planes), min_det, ws, p->tw64, kbase, st);
+  return cuda_status(e);
+}
+
+int lf_lense_flow(lf_plan_t p, const void* f_in, int in_dtype, void* f_out, int out_dtype, const void* planes,
+                  int batch, int nsteps, int direction, int adjoint, void* ws, size_t ws_bytes, void* stream) {
+  if (!p) return LF_ERR_BAD_ARG;
+  if (batch < 0) return LF_ERR_BAD_SHAPE;
+  if ((in_dtype != LF_F32 && in_dtype != LF_F64) || (out_dtype != LF_F32 && out_dtype != LF_F64))
+    return LF_ERR_BAD_DTYPE;
+  if (nsteps < 0 || (direction != LF_FORWARD_LENSE && direction != LF_INVERSE_LENSE)) return LF_ERR_BAD_ARG;
+  if (batch == 0) return LF_OK;
+  if (!f_in || !f_out || !planes || !aligned16(f_in) || !aligned16(f_out) || !aligned16(planes)) return LF_ERR_BAD_ARG;
+  cudaStream_t st = (cudaStream_t)stream;
+  const size_t npix = (size_t)p->N * p->N * (size_t)batch * p->C;
+  if (nsteps == 0) {  // rk4_solve with zero steps returns its input (util.py:199)
+    if (in_dtype != out_dtype) return LF_ERR_BAD_DTYPE;
+    if (f_in == f_out) return LF_OK;
+    return cuda_status(cudaMemcpyAsync(f_out, f_in, npix * (in_dtype == LF_F64 ? 8 : 4), cudaMemcpyDeviceToDevice, st));
+  }
+  const bool adj = adjoint != 0;
+  if (!ws || !aligned16(ws)) return LF_ERR_BAD_ARG;
+  if (ws_bytes < lf_workspace_bytes(p, batch, adj)) return LF_ERR_WORKSPACE;
+  // lense_flow.py:304-322: forward time iff (direction == +1) XOR adjoint
+  const bool fwd_time = ((direction == LF_FORWARD_LENSE) != adj);
+  const double t0 = fwd_time ? 0.0 : 1.0, t1 = fwd_time ? 1.0 : 0.0;
+  const size_t el = p->prec == LF_F64 ? 8 : 4;
+  const size_t plane_bytes = el * npix;
+  StageArgs a;
+  std::memset(&a, 0, sizeof(a));
+  a.f_in = f_in;
+  a.f_out = f_out;
+  a.in_f64 = in_dtype == LF_F64;
+  a.out_f64 = out_dtype == LF_F64;
+  a.phi = planes;
+  char* w = reinterpret_cast<char*>(ws);
+  a.y0 = w;
+  a.acc = w + plane_bytes;
+  a.s = w + 2 * plane_bytes;
+  a.gx = w + 3 * plane_bytes;
+  a.v = adj ? (void*)(w + 4 * plane_bytes) : nullptr;
+  a.twN = p->tw;
+  a.kbase = 2.0 * M_PI / ((double)p->N * p->pix_width);
+  a.nplanes = batch * p->C;
+  cudaError_t e;
+  g_prof = &p->prof;
+  if (p->prec == LF_F64)
+    e = run_lens<double>(p->N, p->C, adj, a, batch, nsteps, t0, t1, st);
+  else
+    e = run_lens<float>(p->N, p->C, adj, a, batch, nsteps, t0, t1, st);
+  return cuda_status(e);
+}
+
+int lf_profile_enable(lf_plan_t p, int enable) {
+  if (!p) return LF_ERR_BAD_ARG;
+  p->prof.on = enable != 0;
+  return LF_OK;
+}
+
+int lf_profile_reset(lf_plan_t p) {
+  if (!p) return LF_ERR_BAD_ARG;
+  p->prof.used = 0;
+  p->prof.kind.clear();
+  return LF_OK;
+}
+
+int lf_profile_read(lf_plan_t p, int kind, double* total_ms, int* launches) {
+  if (!p || !total_ms || !launches) return LF_ERR_BAD_ARG;
+  double tot = 0.0;
+  int n = 0;
+  const size_t nrec = p->prof.kind.size();
+  if (nrec) {
+    cudaError_t e = cudaEventSynchronize(p->prof.pool[2 * nrec - 1]);
+    if (e != cudaSuccess) return cuda_status(e);
+  }
+  for (size_t i = 0; i < nrec; ++i) {
+    if (p->prof.kind[i] != kind) continue;
+    float ms = 0.f;
+    cudaError_t e = cudaEventElapsedTime(&ms, p->prof.pool[2 * i], p->prof.pool[2 * i + 1]);
+    if (e != cudaSuccess) return cuda_status(e);
+    tot += ms;
+    ++n;
+  }
+  *total_ms = tot;
+  *launches = n;
+  return LF_OK;
+}
+
+}  // extern "C"

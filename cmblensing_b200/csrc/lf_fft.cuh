@@ -1,0 +1,326 @@
+// Shared-memory FFT engine for the LenseFlow kernels (sm_100a).
+//
+// A thread block owns a *tile* of LINES independent 1-D transforms ("lines"),
+// each of length L, held in shared memory as complex values laid out
+//
+//     element (m, line)  at  tile[m * LINES + (line ^ (m & (LINES - 1)))]
+//
+// m is the position along the transform axis.  The XOR swizzle makes both
+// access patterns used by the kernels bank-conflict free:
+//   * line-major  (consecutive threads = consecutive lines, same m): the
+//     Stockham passes and the real-FFT pre/post processing;
+//   * row-major   (consecutive threads = consecutive m, same line): the
+//     coalesced global loads/stores of row tiles and the pointwise epilogues.
+//
+// The transforms are radix-R Stockham autosort passes (Govindaraju et al.,
+// "High performance discrete Fourier transforms on graphics processors",
+// SC08): each pass reads R inputs at stride L/R, twiddles, applies a
+// register-resident radix-R DFT and writes in natural order.  Every thread
+// keeps its butterflies' inputs in registers across the pass barrier, so a
+// single buffer suffices.  Twiddles come from a host-computed table
+// tw[e] = exp(-2 pi i e / NTAB) (float64 on the host, rounded once).
+#pragma once
+
+#include <cuda_runtime.h>
+#include <stdint.h>
+
+namespace lf {
+
+template <typename T> struct V2;
+template <> struct V2<float> { using type = float2; };
+template <> struct V2<double> { using type = double2; };
+template <typename T> using c2 = typename V2<T>::type;
+
+template <typename T> __device__ __forceinline__ c2<T> mk(T x, T y) { c2<T> r; r.x = x; r.y = y; return r; }
+template <typename T> __device__ __forceinline__ c2<T> cadd(c2<T> a, c2<T> b) { return mk<T>(a.x + b.x, a.y + b.y); }
+template <typename T> __device__ __forceinline__ c2<T> csub(c2<T> a, c2<T> b) { return mk<T>(a.x - b.x, a.y - b.y); }
+template <typename T> __device__ __forceinline__ c2<T> cmul(c2<T> a, c2<T> b) {
+  return mk<T>(a.x * b.x - a.y * b.y, a.x * b.y + a.y * b.x);
+}
+// a * conj(b)
+template <typename T> __device__ __forceinline__ c2<T> cmulc(c2<T> a, c2<T> b) {
+  return mk<T>(a.x * b.x + a.y * b.y, a.y * b.x - a.x * b.y);
+}
+template <typename T> __device__ __forceinline__ c2<T> cconj(c2<T> a) { return mk<T>(a.x, -a.y); }
+template <typename T> __device__ __forceinline__ c2<T> cscale(c2<T> a, T s) { return mk<T>(a.x * s, a.y * s); }
+// multiply by i
+template <typename T> __device__ __forceinline__ c2<T> cmul_i(c2<T> a) { return mk<T>(-a.y, a.x); }
+
+// Twiddle multiply by exp(-+2 pi i e/NTAB): forward uses tw[e], inverse conj(tw[e]).
+template <typename T, bool INV> __device__ __forceinline__ c2<T> twmul(c2<T> a, c2<T> w) {
+  return INV ? cmulc<T>(a, w) : cmul<T>(a, w);
+}
+
+// x * (-i) for the forward transform, x * (+i) for the inverse.
+template <typename T, bool INV> __device__ __forceinline__ c2<T> rot90(c2<T> a) {
+  return INV ? mk<T>(-a.y, a.x) : mk<T>(a.y, -a.x);
+}
+
+// ----------------------------------------------------------- small DFTs
+// In-place, natural order in and out, unnormalised; forward kernel e^{-2 pi i jk/R}.
+template <typename T, bool INV> __device__ __forceinline__ void dft2(c2<T>* a) {
+  c2<T> t = a[0];
+  a[0] = cadd<T>(t, a[1]);
+  a[1] = csub<T>(t, a[1]);
+}
+
+template <typename T, bool INV> __device__ __forceinline__ void dft4(c2<T>* a) {
+  c2<T> t0 = cadd<T>(a[0], a[2]), t1 = csub<T>(a[0], a[2]);
+  c2<T> t2 = cadd<T>(a[1], a[3]), t3 = rot90<T, INV>(csub<T>(a[1], a[3]));
+  a[0] = cadd<T>(t0, t2);
+  a[2] = csub<T>(t0, t2);
+  a[1] = cadd<T>(t1, t3);
+  a[3] = csub<T>(t1, t3);
+}
+
+// sqrt(2)/2, cos(pi/8), sin(pi/8)
+#define LF_C45 0.70710678118654752440
+#define LF_C22 0.92387953251128675613
+#define LF_S22 0.38268343236508977173
+
+template <typename T, bool INV> __device__ __forceinline__ void dft8(c2<T>* a) {
+  c2<T> e[4] = {a[0], a[2], a[4], a[6]};
+  c2<T> o[4] = {a[1], a[3], a[5], a[7]};
+  dft4<T, INV>(e);
+  dft4<T, INV>(o);
+  const T c = T(LF_C45);
+  // o1 * W8^1, W8^1 = (c, -c) forward / (c, c) inverse
+  c2<T> o1 = INV ? mk<T>(c * (o[1].x - o[1].y), c * (o[1].x + o[1].y))
+                 : mk<T>(c * (o[1].x + o[1].y), c * (o[1].y - o[1].x));
+  c2<T> o2 = rot90<T, INV>(o[2]);
+  // o3 * W8^3, W8^3 = (-c, -c) forward / (-c, c) inverse
+  c2<T> o3 = INV ? mk<T>(-c * (o[3].x + o[3].y), c * (o[3].x - o[3].y))
+                 : mk<T>(c * (o[3].y - o[3].x), -c * (o[3].x + o[3].y));
+  a[0] = cadd<T>(e[0], o[0]);
+  a[4] = csub<T>(e[0], o[0]);
+  a[1] = cadd<T>(e[1], o1);
+  a[5] = csub<T>(e[1], o1);
+  a[2] = cadd<T>(e[2], o2);
+  a[6] = csub<T>(e[2], o2);
+  a[3] = cadd<T>(e[3], o3);
+  a[7] = csub<T>(e[3], o3);
+}
+
+template <typename T, bool INV> __device__ __forceinline__ void dft16(c2<T>* a) {
+  c2<T> e[8], o[8];
+#pragma unroll
+  for (int i = 0; i < 8; ++i) {
+    e[i] = a[2 * i];
+    o[i] = a[2 * i + 1];
+  }
+  dft8<T, INV>(e);
+  dft8<T, INV>(o);
+  // W16^k forward = (cos(pi k/8), -sin(pi k/8)), k = 0..7
+  const T wr[8] = {T(1), T(LF_C22), T(LF_C45), T(LF_S22), T(0), T(-LF_S22), T(-LF_C45), T(-LF_C22)};
+  const T wi[8] = {T(0), T(-LF_S22), T(-LF_C45), T(-LF_C22), T(-1), T(-LF_C22), T(-LF_C45), T(-LF_S22)};
+#pragma unroll
+  for (int k = 0; k < 8; ++k) {
+    c2<T> w = mk<T>(wr[k], INV ? -wi[k] : wi[k]);
+    c2<T> t = (k == 0) ? o[k] : (k == 4 ? rot90<T, INV>(o[k]) : cmul<T>(o[k], w));
+    a[k] = cadd<T>(e[k], t);
+    a[k + 8] = csub<T>(e[k], t);
+  }
+}
+
+template <int R, typename T, bool INV> __device__ __forceinline__ void dft(c2<T>* a) {
+  if constexpr (R == 2) dft2<T, INV>(a);
+  else if constexpr (R == 4) dft4<T, INV>(a);
+  else if constexpr (R == 8) dft8<T, INV>(a);
+  else if constexpr (R == 16) dft16<T, INV>(a);
+  else static_assert(R == 2 || R == 4 || R == 8 || R == 16, "unsupported radix");
+}
+
+// ------------------------------------------------------------ tile layout
+template <int LINES> __device__ __forceinline__ int sw(int m, int line) {
+  return m * LINES + (line ^ (m & (LINES - 1)));
+}
+
+// ------------------------------------------------------------ Stockham pass
+// One radix-R pass over NLINES lines (line l lives in tile (l / LINES) of a
+// sequence of tiles spaced TILE_ELEMS apart) of length L.  NS is the
+// product of the radices of the previous passes.  ``tw`` holds NTAB entries.
+template <typename T, int L, int R, int NS, int LINES, int NTILES, int NT, bool INV, int NTAB>
+__device__ __forceinline__ void stockham_pass(c2<T>* __restrict__ buf, const c2<T>* __restrict__ tw, int tid) {
+  constexpr int NB = L / R;                   // butterflies per line
+  constexpr int TOT = NB * LINES * NTILES;    // butterflies in the pass
+  constexpr int PER = (TOT + NT - 1) / NT;
+  constexpr int TILE_ELEMS = L * LINES;
+  constexpr int TWS = NTAB / (NS * R);        // table stride for W_{NS*R}
+  static_assert(NTAB % (NS * R) == 0, "twiddle table too small");
+  c2<T> v[PER][R];
+#pragma unroll
+  for (int b = 0; b < PER; ++b) {
+    const int idx = tid + b * NT;
+    if (TOT % NT == 0 || idx < TOT) {
+      const int line = idx % LINES;
+      const int rest = idx / LINES;
+      const int j = rest % NB;
+      const int tile = rest / NB;
+      const c2<T>* tb = buf + tile * TILE_ELEMS;
+#pragma unroll
+      for (int r = 0; r < R; ++r) v[b][r] = tb[sw<LINES>(j + r * NB, line)];
+      if constexpr (NS > 1) {
+        const int k = j % NS;
+#pragma unroll
+        for (int r = 1; r < R; ++r) v[b][r] = twmul<T, INV>(v[b][r], tw[r * k * TWS]);
+      }
+      dft<R, T, INV>(v[b]);
+    }
+  }
+  __syncthreads();
+#pragma unroll
+  for (int b = 0; b < PER; ++b) {
+    const int idx = tid + b * NT;
+    if (TOT % NT == 0 || idx < TOT) {
+      const int line = idx % LINES;
+      const int rest = idx / LINES;
+      const int j = rest % NB;
+      const int tile = rest / NB;
+      c2<T>* tb = buf + tile * TILE_ELEMS;
+      const int k = j % NS;
+      const int base = (j / NS) * NS * R + k;
+#pragma unroll
+      for (int r = 0; r < R; ++r) tb[sw<LINES>(base + r * NS, line)] = v[b][r];
+    }
+  }
+  __syncthreads();
+}
+
+// Full transform of length L on NTILES consecutive tiles (LINES lines each).
+// Radix plans: 32 = 8x4, 64 = 8x8, 128 = 8x16, 256 = 16x16, 512 = 8x8x8, 1024 = 16x8x8.
+template <typename T, int L, int LINES, int NTILES, int NT, bool INV, int NTAB>
+__device__ __forceinline__ void fft_tiles(c2<T>* buf, const c2<T>* tw, int tid) {
+  if constexpr (L == 32) {
+    stockham_pass<T, L, 8, 1, LINES, NTILES, NT, INV, NTAB>(buf, tw, tid);
+    stockham_pass<T, L, 4, 8, LINES, NTILES, NT, INV, NTAB>(buf, tw, tid);
+  } else if constexpr (L == 64) {
+    stockham_pass<T, L, 8, 1, LINES, NTILES, NT, INV, NTAB>(buf, tw, tid);
+    stockham_pass<T, L, 8, 8, LINES, NTILES, NT, INV, NTAB>(buf, tw, tid);
+  } else if constexpr (L == 128) {
+    stockham_pass<T, L, 8, 1, LINES, NTILES, NT, INV, NTAB>(buf, tw, tid);
+    stockham_pass<T, L, 16, 8, LINES, NTILES, NT, INV, NTAB>(buf, tw, tid);
+  } else if constexpr (L == 256) {
+    stockham_pass<T, L, 16, 1, LINES, NTILES, NT, INV, NTAB>(buf, tw, tid);
+    stockham_pass<T, L, 16, 16, LINES, NTILES, NT, INV, NTAB>(buf, tw, tid);
+  } else if constexpr (L == 512) {
+    stockham_pass<T, L, 8, 1, LINES, NTILES, NT, INV, NTAB>(buf, tw, tid);
+    stockham_pass<T, L, 8, 8, LINES, NTILES, NT, INV, NTAB>(buf, tw, tid);
+    stockham_pass<T, L, 8, 64, LINES, NTILES, NT, INV, NTAB>(buf, tw, tid);
+  } else if constexpr (L == 1024) {
+    stockham_pass<T, L, 16, 1, LINES, NTILES, NT, INV, NTAB>(buf, tw, tid);
+    stockham_pass<T, L, 8, 16, LINES, NTILES, NT, INV, NTAB>(buf, tw, tid);
+    stockham_pass<T, L, 8, 128, LINES, NTILES, NT, INV, NTAB>(buf, tw, tid);
+  } else {
+    static_assert(L == 32, "unsupported transform length");
+  }
+}
+
+// ----------------------------------------------------- real-FFT packing
+// Rows of N real samples are held as H = N/2 complex values z[m] = x[2m] + i x[2m+1].
+// The packed half spectrum of a row keeps X[k] for 1 <= k < H in slot k and
+// (X[0], X[H]) -- both real for a real row -- as (re, im) of slot 0.
+// twN[k] = exp(-2 pi i k / N).
+
+// After a forward length-H FFT of z: turn Y into the packed spectrum X, in place.
+template <typename T, int H, int LINES, int NTILES, int NT>
+__device__ __forceinline__ void r2c_post(c2<T>* buf, const c2<T>* twN, int tid) {
+  constexpr int ITEMS = (H / 2 + 1) * LINES * NTILES;
+  constexpr int TILE_ELEMS = H * LINES;
+  for (int idx = tid; idx < ITEMS; idx += NT) {
+    const int line = idx % LINES;
+    const int rest = idx / LINES;
+    const int k = rest % (H / 2 + 1);
+    c2<T>* tb = buf + (rest / (H / 2 + 1)) * TILE_ELEMS;
+    if (k == 0) {
+      c2<T> y = tb[sw<LINES>(0, line)];
+      tb[sw<LINES>(0, line)] = mk<T>(y.x + y.y, y.x - y.y);
+    } else {
+      const c2<T> yk = tb[sw<LINES>(k, line)];
+      const c2<T> yc = cconj<T>(tb[sw<LINES>(H - k, line)]);
+      const c2<T> e = cscale<T>(cadd<T>(yk, yc), T(0.5));
+      // O = (yk - yc) / (2i) = -i/2 (yk - yc)
+      const c2<T> d = csub<T>(yk, yc);
+      const c2<T> o = mk<T>(T(0.5) * d.y, T(-0.5) * d.x);
+      const c2<T> wo = cmul<T>(o, twN[k]);
+      tb[sw<LINES>(k, line)] = cadd<T>(e, wo);
+      if (k != H - k) tb[sw<LINES>(H - k, line)] = cconj<T>(csub<T>(e, wo));
+    }
+  }
+  __syncthreads();
+}
+
+// Before an inverse length-H FFT: turn the packed spectrum X into Z, in place,
+// so that IFFT_H(Z) = unnormalised inverse real DFT of X (x[2m] + i x[2m+1]).
+// The imaginary parts of X[0] and X[H] are never used, exactly as irfft does.
+template <typename T, int H, int LINES, int NTILES, int NT>
+__device__ __forceinline__ void c2r_pre(c2<T>* buf, const c2<T>* twN, int tid) {
+  constexpr int ITEMS = (H / 2 + 1) * LINES * NTILES;
+  constexpr int TILE_ELEMS = H * LINES;
+  for (int idx = tid; idx < ITEMS; idx += NT) {
+    const int line = idx % LINES;
+    const int rest = idx / LINES;
+    const int k = rest % (H / 2 + 1);
+    c2<T>* tb = buf + (rest / (H / 2 + 1)) * TILE_ELEMS;
+    if (k == 0) {
+      c2<T> x = tb[sw<LINES>(0, line)];  // (X0, XH)
+      tb[sw<LINES>(0, line)] = mk<T>(x.x + x.y, x.x - x.y);
+    } else {
+      const c2<T> a = tb[sw<LINES>(k, line)];
+      const c2<T> bc = cconj<T>(tb[sw<LINES>(H - k, line)]);
+      const c2<T> p = cadd<T>(a, bc);
+      // q = i * W^{-k} (a - bc), W^{-k} = conj(twN[k])
+      const c2<T> q = cmul_i<T>(cmulc<T>(csub<T>(a, bc), twN[k]));
+      tb[sw<LINES>(k, line)] = cadd<T>(p, q);
+      if (k != H - k) tb[sw<LINES>(H - k, line)] = cconj<T>(csub<T>(p, q));
+    }
+  }
+  __syncthreads();
+}
+
+// -------------------------------------------------- global <-> tile moves
+// Row tile: rows [0, LINES) of a row-major array (row stride ``ld`` elements),
+// elements [0, E) of each row.  Row-major thread mapping: coalesced.
+template <typename T, typename G, int E, int LINES, int NT>
+__device__ __forceinline__ void load_rows(c2<T>* tile, const G* __restrict__ g, long ld, int tid) {
+  for (int idx = tid; idx < E * LINES; idx += NT) {
+    const int row = idx / E, m = idx % E;
+    const G v = g[row * ld + m];
+    tile[sw<LINES>(m, row)] = mk<T>(T(v.x), T(v.y));
+  }
+}
+
+template <typename T, typename G, int E, int LINES, int NT>
+__device__ __forceinline__ void store_rows(G* __restrict__ g, long ld, const c2<T>* tile, int tid) {
+  for (int idx = tid; idx < E * LINES; idx += NT) {
+    const int row = idx / E, m = idx % E;
+    const c2<T> v = tile[sw<LINES>(m, row)];
+    G o;
+    o.x = v.x;
+    o.y = v.y;
+    g[row * ld + m] = o;
+  }
+}
+
+// Column tile: lines [c0, c0+LINES) (clipped to ``ncols``) of an (L x ld)
+// row-major complex array; line-major mapping: coalesced LINES-wide rows.
+template <typename T, int L, int LINES, int NT>
+__device__ __forceinline__ void load_cols(c2<T>* tile, const c2<T>* __restrict__ g, long ld, int c0, int ncols,
+                                          int tid) {
+  for (int idx = tid; idx < L * LINES; idx += NT) {
+    const int m = idx / LINES, line = idx % LINES;
+    const int c = c0 + line;
+    tile[sw<LINES>(m, line)] = (c < ncols) ? g[m * ld + c] : mk<T>(T(0), T(0));
+  }
+}
+
+template <typename T, int L, int LINES, int NT>
+__device__ __forceinline__ void store_cols(c2<T>* __restrict__ g, long ld, int c0, int ncols, const c2<T>* tile,
+                                           int tid) {
+  for (int idx = tid; idx < L * LINES; idx += NT) {
+    const int m = idx / LINES, line = idx % LINES;
+    const int c = c0 + line;
+    if (c < ncols) g[m * ld + c] = tile[sw<LINES>(m, line)];
+  }
+}
+
+}  // namespace lf

@@ -1,0 +1,416 @@
+// LenseFlow kernels: phi-derivative precompute and the two passes of one RK4 stage.
+//
+// Spectral conventions follow the reference exactly (cmb_lensing/util.py:103-137):
+// KX = 2 pi fftfreq(N, d) on axis 0 ("columns" here), KY = 2 pi rfftfreq(N, d)
+// on axis 1 ("rows") with the Nyquist entry negated, and every derivative is
+// irfft2(multiplier * rfft2(.)), whose inverse real transform ignores the
+// imaginary parts of the DC/Nyquist bins of axis 1.
+//
+// Row-spectral arrays ("S", "U", "V", "Gx") hold, for every map row, the
+// packed half spectrum of that row only (axis-1 transform done, axis 0 not):
+// N/2 complex values, slot 0 = (X[0], X[N/2]).  Their N/2 columns are the
+// "lines" of the column pass.  Column 0 -- the packed pair of real sequences
+// X[.,0] and X[.,N/2] -- is transformed as one complex line; multiplying it
+// by the Hermitian-symmetrised multiplier i*KX (zero at KX's Nyquist row)
+// reproduces exactly the real parts that irfft2 keeps for those two columns.
+//
+// d/dx (axis 0) needs the column pass; d/dy (axis 1) is row-local:
+// irfft2(i KY rfft2 f) == per-row irfft(i KY rfft f) because the axis-0
+// transforms cancel.  So one RK4 stage is one column pass + one row pass.
+#pragma once
+
+#include "lf_fft.cuh"
+
+namespace lf {
+
+// ----------------------------------------------------------- parameters
+struct StageArgs {
+  // field I/O (caller dtype: io_f64 ? double : float), [B][C][N][N]
+  const void* f_in;
+  void* f_out;
+  int in_f64, out_f64;
+  // phi derivative planes, [B][5][N][N] of T: phi_x, phi_y, phi_xx, phi_xy, phi_yy
+  const void* phi;
+  // workspace, each [B*C][N*N] T values
+  void* y0;
+  void* acc;
+  void* s;   // standard: rfft_rows(y_s);   adjoint: U = rfft_rows(p_x y_s)
+  void* v;   // adjoint: V = rfft_rows(p_y y_s)
+  void* gx;  // column pass output
+  const void* twN;  // N complex T, exp(-2 pi i k / N)
+  double kbase;     // 2 pi / (N d)
+  double t_cur;     // time of the rate evaluated in this stage
+  double t_next;    // time of the next stage input
+  double h;         // signed step
+  int stage;        // 1..4 (0 = init)
+  int last;         // final stage of the integration
+  int nplanes;      // B*C (column pass)
+};
+
+// p = M(t)^-1 grad(phi) with M = I + t grad grad phi (lense_flow.py:373-381, :398-415)
+template <typename T>
+__device__ __forceinline__ void p_vector(T px, T py, T pxx, T pxy, T pyy, T t, T& ox, T& oy) {
+  const T mxx = T(1) + t * pxx, mxy = t * pxy, myy = T(1) + t * pyy;
+  const T inv = T(1) / (mxx * myy - mxy * mxy + T(1e-12));
+  const T ixx = myy * inv, ixy = -mxy * inv, iyy = mxx * inv;
+  ox = px * ixx + py * ixy;
+  oy = px * ixy + py * iyy;
+}
+
+template <typename T>
+__device__ __forceinline__ c2<T> load_io(const void* p, int f64, long i) {
+  if (f64) {
+    const double2 v = reinterpret_cast<const double2*>(p)[i];
+    return mk<T>(T(v.x), T(v.y));
+  }
+  const float2 v = reinterpret_cast<const float2*>(p)[i];
+  return mk<T>(T(v.x), T(v.y));
+}
+
+template <typename T>
+__device__ __forceinline__ void store_io(void* p, int f64, long i, c2<T> v) {
+  if (f64) {
+    reinterpret_cast<double2*>(p)[i] = make_double2(double(v.x), double(v.y));
+  } else {
+    reinterpret_cast<float2*>(p)[i] = make_float2(float(v.x), float(v.y));
+  }
+}
+
+template <typename T, int N, int NT>
+__device__ __forceinline__ void load_twiddles(c2<T>* tw, const void* g, int tid) {
+  const c2<T>* src = reinterpret_cast<const c2<T>*>(g);
+  for (int i = tid; i < N; i += NT) tw[i] = src[i];
+}
+
+// ======================================================== column pass
+// Gx = IFFT_col( (i KX / N^2) * FFT_col(S) ) on tiles of LINES columns.
+// grid: x = column tile (N/2/LINES), y = plane.
+template <typename T, int N, int LINES, int NT>
+__global__ void __launch_bounds__(NT) k_col(StageArgs a) {
+  constexpr int H = N / 2;
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  c2<T>* tw = reinterpret_cast<c2<T>*>(smem_raw);
+  c2<T>* buf = tw + N;
+  const int tid = threadIdx.x;
+  const int c0 = blockIdx.x * LINES;
+  const long plane = blockIdx.y;
+  load_twiddles<T, N, NT>(tw, a.twN, tid);
+  const c2<T>* in = reinterpret_cast<const c2<T>*>(a.s) + plane * (long)N * H;
+  c2<T>* out = reinterpret_cast<c2<T>*>(a.gx) + plane * (long)N * H;
+  load_cols<T, N, LINES, NT>(buf, in, H, c0, H, tid);
+  __syncthreads();
+  fft_tiles<T, N, LINES, 1, NT, false, N>(buf, tw, tid);
+  const T scale = T(a.kbase / (double(N) * double(N)));
+  for (int idx = tid; idx < N * LINES; idx += NT) {
+    const int m = idx / LINES, line = idx % LINES;
+    const int kx = (m < N / 2) ? m : m - N;
+    T f = scale * T(kx);
+    if (c0 + line == 0 && m == N / 2) f = T(0);  // packed DC/Nyquist line
+    const c2<T> v = buf[sw<LINES>(m, line)];
+    buf[sw<LINES>(m, line)] = mk<T>(-f * v.y, f * v.x);
+  }
+  __syncthreads();
+  fft_tiles<T, N, LINES, 1, NT, true, N>(buf, tw, tid);
+  store_cols<T, N, LINES, NT>(out, H, c0, H, buf, tid);
+}
+
+// ========================================================= row pass
+// One tile = LINES consecutive rows of one map; all C components.
+// Standard RHS (lense_flow.py:365-370):  k = p_x d_x y + p_y d_y y
+// Adjoint RHS  (lense_flow.py:355-362):  k = d_x(p_x y) + d_y(p_y y)
+// RK4 (util.py:184-199): stage 1..3 accumulate k1 + 2 k2 + 2 k3 and form
+// the next stage input; stage 4 forms y0 + h/6 (acc + k4).
+// STAGE0 = true: initialisation (copy the input field, transform the first
+// stage input), no rate evaluation.
+template <typename T, int N, int C, bool ADJ, bool STAGE0, int LINES, int NT>
+__global__ void __launch_bounds__(NT) k_row(StageArgs a) {
+  constexpr int H = N / 2;
+  constexpr long P = (long)N * N;
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  c2<T>* tw = reinterpret_cast<c2<T>*>(smem_raw);
+  c2<T>* buf0 = tw + N;
+  c2<T>* buf1 = buf0 + LINES * H;
+  const int tid = threadIdx.x;
+  const int r0 = blockIdx.x * LINES;
+  const long map = blockIdx.y;
+  load_twiddles<T, N, NT>(tw, a.twN, tid);
+  const T* phi = reinterpret_cast<const T*>(a.phi) + map * 5 * P + (long)r0 * N;
+  const T tnext = T(a.t_next);
+  const T tcur = T(a.t_cur);
+  const T hh = T(a.h);
+  const T ky_scale = T(a.kbase / double(N));
+
+#pragma unroll 1
+  for (int c = 0; c < C; ++c) {
+    const long plane = map * C + c;
+    const long prow = plane * P + (long)r0 * N;  // first pixel of the tile
+    c2<T>* sg = reinterpret_cast<c2<T>*>(a.s) + plane * (N * (long)H) + (long)r0 * H;
+    c2<T>* vg = reinterpret_cast<c2<T>*>(a.v) + plane * (N * (long)H) + (long)r0 * H;
+    const c2<T>* gg = reinterpret_cast<const c2<T>*>(a.gx) + plane * (N * (long)H) + (long)r0 * H;
+    c2<T>* y0g = reinterpret_cast<c2<T>*>(reinterpret_cast<T*>(a.y0) + prow);
+    c2<T>* accg = reinterpret_cast<c2<T>*>(reinterpret_cast<T*>(a.acc) + prow);
+
+    if constexpr (!STAGE0) {
+      // ------------------------------------------ rate from the spectra
+      load_rows<T, c2<T>, H, LINES, NT>(buf0, gg, H, tid);
+      load_rows<T, c2<T>, H, LINES, NT>(buf1, ADJ ? vg : sg, H, tid);
+      __syncthreads();
+      // d_y in the row spectrum: multiply by i KY / N (KY's DC and Nyquist
+      // bins contribute nothing after the inverse real transform).
+      for (int idx = tid; idx < H * LINES; idx += NT) {
+        const int row = idx / H, k = idx % H;
+        const c2<T> w = buf1[sw<LINES>(k, row)];
+        const T f = ky_scale * T(k);
+        const c2<T> dy = (k == 0) ? mk<T>(T(0), T(0)) : mk<T>(-f * w.y, f * w.x);
+        if constexpr (ADJ) {
+          // rate spectrum = Gx + i KY V / N  (one inverse transform)
+          const c2<T> g = buf0[sw<LINES>(k, row)];
+          buf0[sw<LINES>(k, row)] = (k == 0) ? g : cadd<T>(g, dy);
+        } else {
+          buf1[sw<LINES>(k, row)] = dy;
+        }
+      }
+      __syncthreads();
+      constexpr int NTI = ADJ ? 1 : 2;
+      c2r_pre<T, H, LINES, NTI, NT>(buf0, tw, tid);
+      fft_tiles<T, H, LINES, NTI, NT, true, N>(buf0, tw, tid);
+    } else {
+      // --------------------------------------------- initial input
+      const long fo = (map * C + c) * (P / 2) + (long)r0 * H;
+      for (int idx = tid; idx < H * LINES; idx += NT) {
+        const int row = idx / H, m = idx % H;
+        buf0[sw<LINES>(m, row)] = load_io<T>(a.f_in, a.in_f64, fo + (long)row * H + m);
+      }
+      __syncthreads();
+    }
+
+    // ---------------------------------------------- pointwise epilogue
+    for (int idx = tid; idx < H * LINES; idx += NT) {
+      const int row = idx / H, m = idx % H;
+      const long e = (long)row * H + m;  // float2-element index within the tile
+      c2<T> ynext;
+      if constexpr (STAGE0) {
+        ynext = buf0[sw<LINES>(m, row)];
+        y0g[e] = ynext;
+      } else {
+        const c2<T> g0 = buf0[sw<LINES>(m, row)];
+        c2<T> k;
+        if constexpr (ADJ) {
+          k = g0;
+        } else {
+          const c2<T> g1 = buf1[sw<LINES>(m, row)];
+          const c2<T> fx = reinterpret_cast<const c2<T>*>(phi)[e];
+          const c2<T> fy = reinterpret_cast<const c2<T>*>(phi + P)[e];
+          const c2<T> fxx = reinterpret_cast<const c2<T>*>(phi + 2 * P)[e];
+          const c2<T> fxy = reinterpret_cast<const c2<T>*>(phi + 3 * P)[e];
+          const c2<T> fyy = reinterpret_cast<const c2<T>*>(phi + 4 * P)[e];
+          T px, py;
+          p_vector<T>(fx.x, fy.x, fxx.x, fxy.x, fyy.x, tcur, px, py);
+          k.x = px * g0.x + py * g1.x;
+          p_vector<T>(fx.y, fy.y, fxx.y, fxy.y, fyy.y, tcur, px, py);
+          k.y = px * g0.y + py * g1.y;
+        }
+        const c2<T> y0 = y0g[e];
+        if (a.stage == 1) {
+          accg[e] = k;
+          ynext = mk<T>(y0.x + T(0.5) * hh * k.x, y0.y + T(0.5) * hh * k.y);
+        } else if (a.stage == 2) {
+          const c2<T> ac = accg[e];
+          accg[e] = mk<T>(ac.x + T(2) * k.x, ac.y + T(2) * k.y);
+          ynext = mk<T>(y0.x + T(0.5) * hh * k.x, y0.y + T(0.5) * hh * k.y);
+        } else if (a.stage == 3) {
+          const c2<T> ac = accg[e];
+          accg[e] = mk<T>(ac.x + T(2) * k.x, ac.y + T(2) * k.y);
+          ynext = mk<T>(y0.x + hh * k.x, y0.y + hh * k.y);
+        } else {
+          const c2<T> ac = accg[e];
+          const T h6 = hh / T(6);
+          ynext = mk<T>(y0.x + h6 * (ac.x + k.x), y0.y + h6 * (ac.y + k.y));
+          if (a.last) {
+            const long fo = (map * C + c) * (P / 2) + (long)r0 * H;
+            store_io<T>(a.f_out, a.out_f64, fo + e, ynext);
+          } else {
+            y0g[e] = ynext;
+          }
+        }
+      }
+      if (STAGE0 || !a.last) {
+        if constexpr (ADJ) {
+          const c2<T> fx = reinterpret_cast<const c2<T>*>(phi)[e];
+          const c2<T> fy = reinterpret_cast<const c2<T>*>(phi + P)[e];
+          const c2<T> fxx = reinterpret_cast<const c2<T>*>(phi + 2 * P)[e];
+          const c2<T> fxy = reinterpret_cast<const c2<T>*>(phi + 3 * P)[e];
+          const c2<T> fyy = reinterpret_cast<const c2<T>*>(phi + 4 * P)[e];
+          T px0, py0, px1, py1;
+          p_vector<T>(fx.x, fy.x, fxx.x, fxy.x, fyy.x, tnext, px0, py0);
+          p_vector<T>(fx.y, fy.y, fxx.y, fxy.y, fyy.y, tnext, px1, py1);
+          buf0[sw<LINES>(m, row)] = mk<T>(px0 * ynext.x, px1 * ynext.y);
+          buf1[sw<LINES>(m, row)] = mk<T>(py0 * ynext.x, py1 * ynext.y);
+        } else {
+          buf0[sw<LINES>(m, row)] = ynext;
+        }
+      }
+    }
+    __syncthreads();
+    if (!STAGE0 && a.last) continue;  // uniform across the block
+    constexpr int NTO = ADJ ? 2 : 1;
+    fft_tiles<T, H, LINES, NTO, NT, false, N>(buf0, tw, tid);
+    r2c_post<T, H, LINES, NTO, NT>(buf0, tw, tid);
+    store_rows<T, c2<T>, H, LINES, NT>(sg, H, buf0, tid);
+    if constexpr (ADJ) store_rows<T, c2<T>, H, LINES, NT>(vg, H, buf1, tid);
+    __syncthreads();
+  }
+}
+
+// ================================================ phi precompute (FP64)
+// rfft along rows of a real map (N x N double) into the unpacked
+// (N x (N/2+1)) complex layout of rfft2.   grid: x = row tile, y = map.
+template <int N, int LINES, int NT>
+__global__ void __launch_bounds__(NT) k_phi_rows_r2c(const double* __restrict__ phi, double2* __restrict__ out,
+                                                      const double2* __restrict__ twN) {
+  constexpr int H = N / 2;
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  double2* tw = reinterpret_cast<double2*>(smem_raw);
+  double2* buf = tw + N;
+  const int tid = threadIdx.x;
+  const int r0 = blockIdx.x * LINES;
+  const long map = blockIdx.y;
+  load_twiddles<double, N, NT>(tw, twN, tid);
+  const double2* src = reinterpret_cast<const double2*>(phi + map * (long)N * N + (long)r0 * N);
+  load_rows<double, double2, H, LINES, NT>(buf, src, H, tid);
+  __syncthreads();
+  fft_tiles<double, H, LINES, 1, NT, false, N>(buf, tw, tid);
+  r2c_post<double, H, LINES, 1, NT>(buf, tw, tid);
+  double2* dst = out + map * (long)N * (H + 1) + (long)r0 * (H + 1);
+  for (int idx = tid; idx < (H + 1) * LINES; idx += NT) {
+    const int row = idx / (H + 1), k = idx % (H + 1);
+    double2 v;
+    if (k == 0) {
+      v = make_double2(buf[sw<LINES>(0, row)].x, 0.0);
+    } else if (k == H) {
+      v = make_double2(buf[sw<LINES>(0, row)].y, 0.0);
+    } else {
+      v = buf[sw<LINES>(k, row)];
+    }
+    dst[(long)row * (H + 1) + k] = v;
+  }
+}
+
+// In-place forward column FFT of the N/2+1 columns of an (N x (N/2+1)) array.
+template <int N, int LINES, int NT>
+__global__ void __launch_bounds__(NT) k_phi_cols_fwd(double2* __restrict__ arr, const double2* __restrict__ twN) {
+  constexpr int H = N / 2;
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  double2* tw = reinterpret_cast<double2*>(smem_raw);
+  double2* buf = tw + N;
+  const int tid = threadIdx.x;
+  const int c0 = blockIdx.x * LINES;
+  double2* a = arr + blockIdx.y * (long)N * (H + 1);
+  load_twiddles<double, N, NT>(tw, twN, tid);
+  load_cols<double, N, LINES, NT>(buf, a, H + 1, c0, H + 1, tid);
+  __syncthreads();
+  fft_tiles<double, N, LINES, 1, NT, false, N>(buf, tw, tid);
+  store_cols<double, N, LINES, NT>(a, H + 1, c0, H + 1, buf, tid);
+}
+
+// Five derivative spectra: for j in {x, y, xx, xy, yy} apply the multiplier
+// (util.py:125-130), inverse column FFT, and write the packed row spectrum
+// (columns 0 and N/2 keep only their real parts, as irfft2 does).
+// ``spec`` is the unpacked rfft2 of phi; ``packed`` is [B][5][N][N/2] complex.
+template <int N, int LINES, int NT>
+__global__ void __launch_bounds__(NT) k_phi_cols_deriv(const double2* __restrict__ spec, double2* __restrict__ packed,
+                                                        const double2* __restrict__ twN, double kbase) {
+  constexpr int H = N / 2;
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  double2* tw = reinterpret_cast<double2*>(smem_raw);
+  double2* buf = tw + N;
+  const int tid = threadIdx.x;
+  const int c0 = blockIdx.x * LINES;
+  const long map = blockIdx.y;
+  const double2* a = spec + map * (long)N * (H + 1);
+  load_twiddles<double, N, NT>(tw, twN, tid);
+  const double scale = 1.0 / (double(N) * double(N));
+#pragma unroll 1
+  for (int j = 0; j < 5; ++j) {
+    load_cols<double, N, LINES, NT>(buf, a, H + 1, c0, H + 1, tid);
+    __syncthreads();
+    for (int idx = tid; idx < N * LINES; idx += NT) {
+      const int m = idx / LINES, line = idx % LINES;
+      const int col = c0 + line;
+      const double kx = kbase * double(m < N / 2 ? m : m - N);
+      const double ky = (col == H) ? -kbase * double(H) : kbase * double(col);
+      const double2 v = buf[sw<LINES>(m, line)];
+      double2 r;
+      if (j == 0) r = make_double2(-kx * v.y * scale, kx * v.x * scale);
+      else if (j == 1) r = make_double2(-ky * v.y * scale, ky * v.x * scale);
+      else {
+        const double f = (j == 2 ? -kx * kx : (j == 3 ? -kx * ky : -ky * ky)) * scale;
+        r = make_double2(f * v.x, f * v.y);
+      }
+      buf[sw<LINES>(m, line)] = r;
+    }
+    __syncthreads();
+    fft_tiles<double, N, LINES, 1, NT, true, N>(buf, tw, tid);
+    double2* out = packed + (map * 5 + j) * (long)N * H;
+    for (int idx = tid; idx < N * LINES; idx += NT) {
+      const int m = idx / LINES, line = idx % LINES;
+      const int col = c0 + line;
+      const double2 v = buf[sw<LINES>(m, line)];
+      if (col == 0) reinterpret_cast<double*>(out + (long)m * H)[0] = v.x;
+      else if (col == H) reinterpret_cast<double*>(out + (long)m * H)[1] = v.x;
+      else if (col < H) out[(long)m * H + col] = v;
+    }
+    __syncthreads();
+  }
+}
+
+// Inverse real transform of the packed rows into the five derivative planes.
+// grid: x = row tile, y = map * 5 + j.
+template <typename TO, int N, int LINES, int NT>
+__global__ void __launch_bounds__(NT) k_phi_rows_c2r(const double2* __restrict__ packed, TO* __restrict__ planes,
+                                                      const double2* __restrict__ twN) {
+  constexpr int H = N / 2;
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  double2* tw = reinterpret_cast<double2*>(smem_raw);
+  double2* buf = tw + N;
+  const int tid = threadIdx.x;
+  const int r0 = blockIdx.x * LINES;
+  const long pl = blockIdx.y;
+  load_twiddles<double, N, NT>(tw, twN, tid);
+  load_rows<double, double2, H, LINES, NT>(buf, packed + pl * (long)N * H + (long)r0 * H, H, tid);
+  __syncthreads();
+  c2r_pre<double, H, LINES, 1, NT>(buf, tw, tid);
+  fft_tiles<double, H, LINES, 1, NT, true, N>(buf, tw, tid);
+  using O2 = c2<TO>;
+  O2* dst = reinterpret_cast<O2*>(planes + pl * (long)N * N + (long)r0 * N);
+  store_rows<double, O2, H, LINES, NT>(dst, H, buf, tid);
+}
+
+// Per-map minimum over pixels and t in [0, 1] of det(I + t grad grad phi).
+__device__ __forceinline__ int ordered_int(float f) {
+  const int i = __float_as_int(f);
+  return i >= 0 ? i : i ^ 0x7fffffff;
+}
+
+template <typename T>
+__global__ void k_min_det(const T* __restrict__ planes, long P, int* __restrict__ out) {
+  const long map = blockIdx.y;
+  const T* pxx = planes + map * 5 * P + 2 * P;
+  const T* pxy = pxx + P;
+  const T* pyy = pxy + P;
+  double best = 1.0;
+  for (long i = blockIdx.x * (long)blockDim.x + threadIdx.x; i < P; i += (long)gridDim.x * blockDim.x) {
+    const double A = pxx[i], B = pxy[i], Cc = pyy[i];
+    const double q = A * Cc - B * B, l = A + Cc;
+    double d = 1.0 + l + q;  // t = 1
+    if (q > 0.0) {
+      const double ts = -l / (2.0 * q);
+      if (ts > 0.0 && ts < 1.0) d = fmin(d, 1.0 + ts * l + ts * ts * q);
+    }
+    best = fmin(best, d);
+  }
+  for (int o = 16; o > 0; o >>= 1) best = fmin(best, __shfl_xor_sync(0xffffffffu, best, o));
+  if ((threadIdx.x & 31) == 0) atomicMin(out + map, ordered_int(float(best)));
+}
+
+}  // namespace lf

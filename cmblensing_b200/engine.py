@@ -1,0 +1,209 @@
+"""Device-level LenseFlow API on torch CUDA tensors (batched, stream-aware).
+
+torch only supplies device memory and the current stream; all arithmetic runs
+in the CUDA kernels of liblenseflow.so, reached through the C ABI.
+"""
+from __future__ import annotations
+
+import ctypes
+import threading
+
+import torch
+
+from . import _native as nat
+from .constants import FORWARD_LENSE, INVERSE_LENSE
+
+_plans = {}
+_plans_lock = threading.Lock()
+
+
+def _stream_ptr(device):
+    return ctypes.c_void_p(torch.cuda.current_stream(device).cuda_stream)
+
+
+def _ptr(t):
+    return ctypes.c_void_p(t.data_ptr())
+
+
+class Plan:
+    """A plan for N x N maps with C components in float32 or float64 compute."""
+
+    def __init__(self, nside, ncomp, pix_width, precision="f32", device=None):
+        lib = nat.load()
+        self.nside = int(nside)
+        self.ncomp = int(ncomp)
+        self.pix_width = float(pix_width)
+        self.precision = precision
+        self.prec_code = nat.LF_F64 if precision == "f64" else nat.LF_F32
+        self.dtype = torch.float64 if precision == "f64" else torch.float32
+        self.device = torch.device("cuda", torch.cuda.current_device() if device is None else torch.device(device).index)
+        h = ctypes.c_void_p()
+        with torch.cuda.device(self.device):
+            nat.check(lib.lf_plan_create(ctypes.byref(h), self.nside, self.ncomp, self.pix_width, self.prec_code),
+                      "lf_plan_create")
+        self.handle = h
+        self._lib = lib
+
+    def __del__(self):
+        try:
+            if getattr(self, "handle", None) and self.handle.value:
+                self._lib.lf_plan_destroy(self.handle)
+        except Exception:
+            pass
+
+    # -------------------------------------------------------------- sizes
+    def workspace_bytes(self, batch, adjoint):
+        return int(self._lib.lf_workspace_bytes(self.handle, int(batch), int(bool(adjoint))))
+
+    def phi_planes_bytes(self, batch):
+        return int(self._lib.lf_phi_planes_bytes(self.handle, int(batch)))
+
+    def phi_workspace_bytes(self, batch):
+        return int(self._lib.lf_phi_workspace_bytes(self.handle, int(batch)))
+
+    # ------------------------------------------------------------ phi
+    def phi_planes(self, phi, check_det=True, out=None, workspace=None):
+        """phi: [B,N,N] float64 map or [B,N,N/2+1] complex128 Fourier (rfft2 layout), on this device.
+
+        Returns the [B,5,N,N] derivative planes in the plan's precision.  With
+        ``check_det`` the minimum over pixels and t in [0,1] of
+        det(I + t grad grad phi) is read back and a SingularMagnificationError
+        raised if it is not positive (one device sync).
+        """
+        N = self.nside
+        if phi.dim() == 2:
+            phi = phi.unsqueeze(0)
+        if phi.shape[-2:] == (N, N):
+            basis = nat.LF_PHI_MAP
+            phi = phi.to(device=self.device, dtype=torch.float64).contiguous()
+        elif phi.shape[-2:] == (N, N // 2 + 1):
+            basis = nat.LF_PHI_FOURIER
+            phi = phi.to(device=self.device, dtype=torch.complex128).contiguous()
+        else:
+            raise nat.LenseFlowError(nat.LF_ERR_BAD_SHAPE, f"phi shape {tuple(phi.shape)} for N={N}")
+        B = phi.shape[0]
+        planes = out if out is not None else torch.empty((B, 5, N, N), dtype=self.dtype, device=self.device)
+        if planes.shape != (B, 5, N, N) or planes.dtype != self.dtype or not planes.is_contiguous():
+            raise nat.LenseFlowError(nat.LF_ERR_BAD_SHAPE, "phi plane buffer does not match")
+        ws = workspace
+        if ws is None or ws.numel() < self.phi_workspace_bytes(B):
+            ws = torch.empty(max(self.phi_workspace_bytes(B), 16), dtype=torch.uint8, device=self.device)
+        md = torch.empty(max(B, 1), dtype=torch.int32, device=self.device) if check_det else None
+        with torch.cuda.device(self.device):
+            st = _stream_ptr(self.device)
+            if md is not None:
+                nat.check(self._lib.lf_min_det_init(_ptr(md), B, st), "lf_min_det_init")
+            nat.check(self._lib.lf_phi_precompute(self.handle, _ptr(phi), basis, B, _ptr(planes),
+                                                  _ptr(md) if md is not None else None, _ptr(ws), ws.numel(), st),
+                      "lf_phi_precompute")
+        if md is not None:
+            vals = [self._lib.lf_decode_min_det(int(v)) for v in md.cpu().tolist()[:B]]
+            self.last_min_det = vals
+            if not all(v > 0.0 for v in vals):
+                raise nat.SingularMagnificationError(nat.LF_ERR_SINGULAR_MAGNIFICATION,
+                                                     f"min det(I + t grad grad phi) = {min(vals):.3g}")
+        return planes
+
+    # ------------------------------------------------------------ lens
+    def lense_flow(self, f, planes, n=10, direction=FORWARD_LENSE, adjoint=False, out=None, workspace=None,
+                   out_dtype=None):
+        """f: [B,C,N,N] float32/float64 map-space fields on this device (C = plan's ncomp)."""
+        N, C = self.nside, self.ncomp
+        if f.dim() != 4 or f.shape[1:] != (C, N, N):
+            raise nat.LenseFlowError(nat.LF_ERR_BAD_SHAPE, f"field shape {tuple(f.shape)} for C={C}, N={N}")
+        if f.dtype not in (torch.float32, torch.float64):
+            raise nat.LenseFlowError(nat.LF_ERR_BAD_DTYPE, str(f.dtype))
+        f = f.contiguous()
+        B = f.shape[0]
+        if planes.shape != (B, 5, N, N) or planes.dtype != self.dtype or not planes.is_contiguous():
+            raise nat.LenseFlowError(nat.LF_ERR_BAD_SHAPE, "phi planes do not match the field batch / plan")
+        odt = f.dtype if out_dtype is None else out_dtype
+        if out is None:
+            out = torch.empty((B, C, N, N), dtype=odt, device=self.device)
+        need = self.workspace_bytes(B, adjoint)
+        if workspace is None or workspace.numel() < need:
+            workspace = torch.empty(max(need, 16), dtype=torch.uint8, device=self.device)
+        code = lambda t: nat.LF_F64 if t == torch.float64 else nat.LF_F32
+        with torch.cuda.device(self.device):
+            nat.check(self._lib.lf_lense_flow(self.handle, _ptr(f), code(f.dtype), _ptr(out), code(out.dtype),
+                                              _ptr(planes), B, int(n), int(direction), int(bool(adjoint)),
+                                              _ptr(workspace), workspace.numel(), _stream_ptr(self.device)),
+                      "lf_lense_flow")
+        return out
+
+
+    # ---------------------------------------------------------- profiling
+    def profile(self, enable=True):
+        nat.check(self._lib.lf_profile_enable(self.handle, int(bool(enable))), "lf_profile_enable")
+
+    def profile_reset(self):
+        nat.check(self._lib.lf_profile_reset(self.handle), "lf_profile_reset")
+
+    def profile_read(self, kind):
+        """(total milliseconds, launch count) of the recorded launches of one kernel kind."""
+        ms = ctypes.c_double()
+        n = ctypes.c_int()
+        nat.check(self._lib.lf_profile_read(self.handle, int(kind), ctypes.byref(ms), ctypes.byref(n)),
+                  "lf_profile_read")
+        return ms.value, n.value
+
+
+class HostPipeline:
+    """The reference-facing call with host buffers, for a fixed batch.
+
+    Each call copies f [B,C,N,N] and phi [B,N,N] (float64, pinned host) to the
+    device, computes the phi derivative planes (with the magnification check),
+    lenses, and copies the result back into a pinned host buffer.  Device
+    buffers are allocated once.
+    """
+
+    def __init__(self, plan, batch, io_dtype=torch.float64):
+        self.plan = plan
+        N, C = plan.nside, plan.ncomp
+        dev = plan.device
+        self.batch = batch
+        self.d_f = torch.empty((batch, C, N, N), dtype=io_dtype, device=dev)
+        self.d_out = torch.empty_like(self.d_f)
+        self.d_phi = torch.empty((batch, N, N), dtype=torch.float64, device=dev)
+        self.planes = torch.empty((batch, 5, N, N), dtype=plan.dtype, device=dev)
+        self.ws = torch.empty(max(plan.workspace_bytes(batch, True), 16), dtype=torch.uint8, device=dev)
+        self.phi_ws = torch.empty(max(plan.phi_workspace_bytes(batch), 16), dtype=torch.uint8, device=dev)
+
+    def h2d_bytes(self):
+        return self.d_f.numel() * self.d_f.element_size() + self.d_phi.numel() * 8
+
+    def d2h_bytes(self):
+        return self.d_out.numel() * self.d_out.element_size()
+
+    def __call__(self, f_host, phi_host, out_host, n=10, direction=FORWARD_LENSE, adjoint=False, check_det=True):
+        self.d_f.copy_(f_host, non_blocking=True)
+        self.d_phi.copy_(phi_host, non_blocking=True)
+        self.plan.phi_planes(self.d_phi, check_det=check_det, out=self.planes, workspace=self.phi_ws)
+        self.plan.lense_flow(self.d_f, self.planes, n=n, direction=direction, adjoint=adjoint, out=self.d_out,
+                             workspace=self.ws)
+        out_host.copy_(self.d_out, non_blocking=True)
+        return out_host
+
+
+def get_plan(nside, ncomp, pix_width, precision="f32", device=None):
+    dev = torch.cuda.current_device() if device is None else torch.device(device).index
+    key = (dev, int(nside), int(ncomp), float(pix_width), precision)
+    with _plans_lock:
+        p = _plans.get(key)
+        if p is None:
+            p = Plan(nside, ncomp, pix_width, precision, device=torch.device("cuda", dev))
+            _plans[key] = p
+        return p
+
+
+def lense_flow_batch(f, phi, pix_width, n=10, direction=FORWARD_LENSE, adjoint=False, precision="f32",
+                     check_det=True):
+    """Batched LenseFlow on device tensors: f [B,C,N,N], phi [B,N,N] map or [B,N,N/2+1] Fourier."""
+    if f.dim() == 3:
+        f = f.unsqueeze(0)
+    plan = get_plan(f.shape[-1], f.shape[1], pix_width, precision, device=f.device)
+    planes = plan.phi_planes(phi, check_det=check_det)
+    return plan.lense_flow(f, planes, n=n, direction=direction, adjoint=adjoint)
+
+
+__all__ = ["Plan", "HostPipeline", "get_plan", "lense_flow_batch", "FORWARD_LENSE", "INVERSE_LENSE"]

@@ -1,0 +1,106 @@
+/* LenseFlow engine for B200 (sm_100a): C ABI.
+ *
+ * Plain pointers and sizes only.  Every device pointer is caller-owned and
+ * must be 16-byte aligned; the library never frees caller memory.  Every call
+ * that launches work takes a cudaStream_t passed as ``void*`` (NULL = the
+ * legacy default stream) and is asynchronous with respect to the host.
+ *
+ * Layouts (row-major, as in zaneblood1/CMBLensing.py):
+ *   field  : [batch][ncomp][N][N]          map basis, float32 or float64
+ *            (ncomp 1 = T, 2 = Q,U, 3 = T,Q,U -- the matrices of FlatS0 /
+ *             FlatS2 / FlatS02, cmb_lensing/fields.py:81-116)
+ *   phi    : [batch][N][N] float64 map, or [batch][N][N/2+1] complex128
+ *            (interleaved re,im) Fourier = unnormalised rfft2 layout
+ *   planes : [batch][5][N][N] in the plan's precision: d_x phi, d_y phi,
+ *            d_xx phi, d_xy phi, d_yy phi (cmb_lensing/util.py:110-130)
+ *
+ * Status codes are returned, never raised; nothing aborts or traps.
+ */
+#ifndef LENSEFLOW_H
+#define LENSEFLOW_H
+
+#include <stddef.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+enum lf_status {
+  LF_OK = 0,
+  LF_ERR_BAD_SHAPE = 1,
+  LF_ERR_BAD_DTYPE = 2,
+  LF_ERR_BAD_ARG = 3,
+  LF_ERR_SINGULAR_MAGNIFICATION = 4,
+  LF_ERR_OOM = 5,
+  LF_ERR_TIMEOUT = 6,
+  LF_ERR_CUDA = 7,
+  LF_ERR_WORKSPACE = 8
+};
+
+enum lf_dtype { LF_F32 = 0, LF_F64 = 1 };
+enum lf_phi_basis { LF_PHI_MAP = 0, LF_PHI_FOURIER = 1 };
+
+/* Direction constants of cmb_lensing/constants.py:7-8. */
+#define LF_FORWARD_LENSE 1
+#define LF_INVERSE_LENSE (-1)
+
+typedef struct lf_plan_s* lf_plan_t;
+
+/* Library version (major*10000 + minor*100 + patch). */
+int lf_version(void);
+
+/* Human-readable name of a status code (static string). */
+const char* lf_status_string(int status);
+
+/* Create a plan for N x N maps with ``ncomp`` components, pixel width
+ * ``pix_width`` in radians (fields.py:21, lense_flow.py:291) and compute
+ * precision LF_F32 or LF_F64.  N must be one of 64, 128, 256, 512, 1024.
+ * Allocates only the plan's twiddle tables on the current device.
+ * Replaces the per-call setup of lense_flow (cmb_lensing/lense_flow.py:289-302). */
+int lf_plan_create(lf_plan_t* plan, int nside, int ncomp, double pix_width, int precision);
+int lf_plan_destroy(lf_plan_t plan);
+
+/* Bytes of caller workspace needed by lf_lense_flow for ``batch`` maps. */
+size_t lf_workspace_bytes(lf_plan_t plan, int batch, int adjoint);
+/* Bytes of the derivative-plane buffer for ``batch`` maps. */
+size_t lf_phi_planes_bytes(lf_plan_t plan, int batch);
+/* Bytes of float64 scratch needed by lf_phi_precompute for ``batch`` maps. */
+size_t lf_phi_workspace_bytes(lf_plan_t plan, int batch);
+
+/* d_x, d_y, d_xx, d_xy, d_yy of phi, computed in float64 and stored in the
+ * plan's precision.  Replaces get_primal_derivatives /
+ * get_primal_derivatives_from_fourier (cmb_lensing/util.py:110-130) as used
+ * by primal_lense_flow (cmb_lensing/lense_flow.py:299-302).
+ * If ``min_det`` (device, ``batch`` ints) is non-NULL it receives, per map,
+ * min over pixels and t in [0,1] of det(I + t grad grad phi), encoded with
+ * lf_decode_min_det; the caller must initialise it with lf_min_det_init. */
+int lf_phi_precompute(lf_plan_t plan, const void* phi, int phi_basis, int batch, void* planes, int* min_det,
+                      void* workspace, size_t workspace_bytes, void* stream);
+int lf_min_det_init(int* min_det, int batch, void* stream);
+float lf_decode_min_det(int encoded);
+
+/* LenseFlow: RK4 with ``nsteps`` fixed steps of df/dt = grad(phi)^T M^-1 grad f
+ * (adjoint = 0) or df/dt = div(M^-1 grad(phi) f) (adjoint = 1), time running
+ * 0 -> 1 iff (direction == +1) XOR adjoint.  Replaces lense_flow /
+ * primal_lense_flow / single_lense_flow_step (cmb_lensing/lense_flow.py:289-352)
+ * for all ``ncomp`` components of ``batch`` maps.  f_in may equal f_out.
+ * ``in_dtype``/``out_dtype`` select float32/float64 field I/O. */
+int lf_lense_flow(lf_plan_t plan, const void* f_in, int in_dtype, void* f_out, int out_dtype, const void* planes,
+                  int batch, int nsteps, int direction, int adjoint, void* workspace, size_t workspace_bytes,
+                  void* stream);
+
+/* Launch timing for benchmarks and profiling.  While enabled, every kernel
+ * launched through ``plan`` is bracketed by a CUDA event pair on its stream.
+ * lf_profile_read synchronises on the last event and returns the summed
+ * duration and count of the recorded launches of one kind.  No counterpart
+ * in the reference (its device work is XLA-generated). */
+enum lf_kernel_kind { LF_KIND_ROW = 0, LF_KIND_COL = 1, LF_KIND_PHI = 2 };
+int lf_profile_enable(lf_plan_t plan, int enable);
+int lf_profile_reset(lf_plan_t plan);
+int lf_profile_read(lf_plan_t plan, int kind, double* total_ms, int* launches);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* LENSEFLOW_H */
