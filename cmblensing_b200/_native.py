@@ -42,6 +42,11 @@ SIGNATURES = {
     "lf_min_det_init": (_i, [_vp, _i, _vp]),
     "lf_decode_min_det": (ctypes.c_float, [_i]),
     "lf_lense_flow": (_i, [_vp, _vp, _i, _vp, _i, _vp, _i, _i, _i, _i, _vp, _sz, _vp]),
+    "lf_fft_workspace_bytes": (_sz, [_vp, _i]),
+    "lf_rfft2": (_i, [_vp, _vp, _i, _i, _vp, _vp]),
+    "lf_irfft2": (_i, [_vp, _vp, _i, _vp, _i, _vp, _sz, _vp]),
+    "lf_vjp_workspace_bytes": (_sz, [_vp, _i]),
+    "lf_lense_flow_vjp": (_i, [_vp, _vp, _vp, _i, _vp, _i, _i, _i, _vp, _vp, _vp, _i, _vp, _sz, _vp]),
     "lf_profile_enable": (_i, [_vp, _i]),
     "lf_profile_reset": (_i, [_vp]),
     "lf_profile_read": (_i, [_vp, _i, ctypes.POINTER(ctypes.c_double), ctypes.POINTER(_i)]),

@@ -2,6 +2,7 @@
 #include <cuda_runtime.h>
 #include <stdint.h>
 
+#include <algorithm>
 #include <cmath>
 #include <cstring>
 #include <new>
@@ -204,6 +205,153 @@ cudaError_t run_phi(int N, const void* phi, int basis, int B, TO* planes, int* m
   }
 }
 
+// --------------------------------------------------- float64 rfft2 / irfft2
+template <int N>
+cudaError_t run_rfft2_n(const void* maps, int in_f64, int B, double2* spec, const double2* tw64, cudaStream_t st) {
+  constexpr int LINES = 8;
+  constexpr int NT = Geo<double>::nt(N);
+  constexpr int H = N / 2;
+  const size_t smem_row = sizeof(double2) * (N + LINES * H);
+  const size_t smem_col = sizeof(double2) * (N + LINES * N);
+  const int ctiles = (H + 1 + LINES - 1) / LINES;
+  cudaError_t e;
+  if (in_f64)
+    e = launch<k_phi_rows_r2c<N, LINES, NT, double>>(dim3(N / LINES, B), NT, smem_row, st,
+                                                     reinterpret_cast<const double*>(maps), spec, tw64);
+  else
+    e = launch<k_phi_rows_r2c<N, LINES, NT, float>>(dim3(N / LINES, B), NT, smem_row, st,
+                                                    reinterpret_cast<const float*>(maps), spec, tw64);
+  if (e != cudaSuccess) return e;
+  return launch<k_phi_cols_fwd<N, LINES, NT>>(dim3(ctiles, B), NT, smem_col, st, spec, tw64);
+}
+
+template <int N>
+cudaError_t run_irfft2_n(const double2* spec, int B, void* maps, int out_f64, double2* packed, const double2* tw64,
+                         cudaStream_t st) {
+  constexpr int LINES = 8;
+  constexpr int NT = Geo<double>::nt(N);
+  constexpr int H = N / 2;
+  const size_t smem_row = sizeof(double2) * (N + LINES * H);
+  const size_t smem_col = sizeof(double2) * (N + LINES * N);
+  const int ctiles = (H + 1 + LINES - 1) / LINES;
+  cudaError_t e = launch<k_spec_cols_inv<N, LINES, NT>>(dim3(ctiles, B), NT, smem_col, st, spec, packed, tw64);
+  if (e != cudaSuccess) return e;
+  if (out_f64)
+    return launch<k_phi_rows_c2r<double, N, LINES, NT>>(dim3(N / LINES, B), NT, smem_row, st, (const double2*)packed,
+                                                        reinterpret_cast<double*>(maps), tw64);
+  return launch<k_phi_rows_c2r<float, N, LINES, NT>>(dim3(N / LINES, B), NT, smem_row, st, (const double2*)packed,
+                                                     reinterpret_cast<float*>(maps), tw64);
+}
+
+cudaError_t run_rfft2(int N, const void* maps, int in_f64, int B, double2* spec, const double2* tw64, cudaStream_t st) {
+  switch (N) {
+    case 64: return run_rfft2_n<64>(maps, in_f64, B, spec, tw64, st);
+    case 128: return run_rfft2_n<128>(maps, in_f64, B, spec, tw64, st);
+    case 256: return run_rfft2_n<256>(maps, in_f64, B, spec, tw64, st);
+    case 512: return run_rfft2_n<512>(maps, in_f64, B, spec, tw64, st);
+    default: return run_rfft2_n<1024>(maps, in_f64, B, spec, tw64, st);
+  }
+}
+
+cudaError_t run_irfft2(int N, const double2* spec, int B, void* maps, int out_f64, double2* packed,
+                       const double2* tw64, cudaStream_t st) {
+  switch (N) {
+    case 64: return run_irfft2_n<64>(spec, B, maps, out_f64, packed, tw64, st);
+    case 128: return run_irfft2_n<128>(spec, B, maps, out_f64, packed, tw64, st);
+    case 256: return run_irfft2_n<256>(spec, B, maps, out_f64, packed, tw64, st);
+    case 512: return run_irfft2_n<512>(spec, B, maps, out_f64, packed, tw64, st);
+    default: return run_irfft2_n<1024>(spec, B, maps, out_f64, packed, tw64, st);
+  }
+}
+
+// ------------------------------------------------------------------ VJP
+// Workspace of lf_lense_flow_vjp, in order.
+struct VjpLayout {
+  size_t f_sys, d_sys, grad, dsave, fback, dacc, spec, dphi_f, total;
+  VjpLayout(int N, int C, int B, size_t el) {
+    const size_t bcp = (size_t)B * C * N * N, bp = (size_t)B * N * N, half = (size_t)B * N * (N / 2 + 1);
+    f_sys = 4 * el * bcp;
+    d_sys = 5 * el * bcp;
+    grad = 2 * el * bcp;
+    dsave = el * bcp;
+    fback = 8 * bcp;
+    dacc = 5 * 8 * bp;
+    spec = 5 * 16 * half;
+    dphi_f = 16 * half;
+    total = f_sys + d_sys + grad + dsave + fback + dacc + spec + dphi_f;
+  }
+};
+
+template <typename T, int N, int C>
+cudaError_t run_vjp_n(const StageArgs& af0, const StageArgs& ad0, double* dacc, int B, int nsteps, double t0,
+                      double t1, cudaStream_t st) {
+  constexpr int LINES = Geo<T>::LINES;
+  constexpr int NT = Geo<T>::nt(N);
+  constexpr int H = N / 2;
+  const size_t smem_row = sizeof(c2<T>) * (N + 2 * LINES * H);
+  const size_t smem_col = sizeof(c2<T>) * (N + LINES * N);
+  const dim3 grow(N / LINES, B);
+  const dim3 gcol(H / LINES, B * C);
+  const long P = (long)N * N;
+  const int gacc = (int)std::min<long>(((long)B * P + 255) / 256, 4096);
+  StageArgs af = af0, ad = ad0;
+  const double h = (t1 - t0) / nsteps;
+  const double hh = h / 2.0;
+  const double cw[4] = {1.0, 2.0, 2.0, 1.0};
+  af.h = ad.h = h;
+  af.stage = ad.stage = 0;
+  af.last = ad.last = 0;
+  af.t_cur = af.t_next = ad.t_cur = ad.t_next = t0;
+  cudaError_t e = launch_k<k_row<T, N, C, false, true, LINES, NT, false>>(LF_KIND_ROW, grow, NT, smem_row, st, af);
+  if (e != cudaSuccess) return e;
+  e = launch_k<k_row<T, N, C, true, true, LINES, NT, true>>(LF_KIND_ROW, grow, NT, smem_row, st, ad);
+  if (e != cudaSuccess) return e;
+  for (int i = 0; i < nsteps; ++i) {
+    const double t = t0 + i * h;
+    const double tc[4] = {t, t + hh, t + hh, t + h};
+    const double tn[4] = {t + hh, t + hh, t + h, t0 + (i + 1) * h};
+    for (int s = 0; s < 4; ++s) {
+      const int last = (i == nsteps - 1 && s == 3);
+      af.stage = ad.stage = s + 1;
+      af.t_cur = ad.t_cur = tc[s];
+      af.t_next = ad.t_next = tn[s];
+      af.last = ad.last = last;
+      e = launch_k<k_col<T, N, LINES, NT>>(LF_KIND_COL, gcol, NT, smem_col, st, af);
+      if (e != cudaSuccess) return e;
+      e = launch_k<k_row<T, N, C, false, false, LINES, NT, true>>(LF_KIND_ROW, grow, NT, smem_row, st, af);
+      if (e != cudaSuccess) return e;
+      e = launch<k_dphi_accum<T, C>>(dim3(gacc), 256, 0, st, (const T*)af.grad, (const T*)ad.dsave,
+                                     (const T*)af.phi, dacc, B, P, tc[s], h / 6.0 * cw[s], (int)(i == 0 && s == 0));
+      if (e != cudaSuccess) return e;
+      e = launch_k<k_col<T, N, LINES, NT>>(LF_KIND_COL, gcol, NT, smem_col, st, ad);
+      if (e != cudaSuccess) return e;
+      e = launch_k<k_row<T, N, C, true, false, LINES, NT, true>>(LF_KIND_ROW, grow, NT, smem_row, st, ad);
+      if (e != cudaSuccess) return e;
+    }
+  }
+  return cudaSuccess;
+}
+
+template <typename T, int N>
+cudaError_t run_vjp_c(int C, const StageArgs& af, const StageArgs& ad, double* dacc, int B, int nsteps, double t0,
+                      double t1, cudaStream_t st) {
+  if (C == 1) return run_vjp_n<T, N, 1>(af, ad, dacc, B, nsteps, t0, t1, st);
+  if (C == 2) return run_vjp_n<T, N, 2>(af, ad, dacc, B, nsteps, t0, t1, st);
+  return run_vjp_n<T, N, 3>(af, ad, dacc, B, nsteps, t0, t1, st);
+}
+
+template <typename T>
+cudaError_t run_vjp(int N, int C, const StageArgs& af, const StageArgs& ad, double* dacc, int B, int nsteps,
+                    double t0, double t1, cudaStream_t st) {
+  switch (N) {
+    case 64: return run_vjp_c<T, 64>(C, af, ad, dacc, B, nsteps, t0, t1, st);
+    case 128: return run_vjp_c<T, 128>(C, af, ad, dacc, B, nsteps, t0, t1, st);
+    case 256: return run_vjp_c<T, 256>(C, af, ad, dacc, B, nsteps, t0, t1, st);
+    case 512: return run_vjp_c<T, 512>(C, af, ad, dacc, B, nsteps, t0, t1, st);
+    default: return run_vjp_c<T, 1024>(C, af, ad, dacc, B, nsteps, t0, t1, st);
+  }
+}
+
 bool aligned16(const void* p) { return (reinterpret_cast<uintptr_t>(p) & 15u) == 0; }
 
 }  // namespace
@@ -371,6 +519,111 @@ int lf_lense_flow(lf_plan_t p, const void* f_in, int in_dtype, void* f_out, int 
     e = run_lens<double>(p->N, p->C, adj, a, batch, nsteps, t0, t1, st);
   else
     e = run_lens<float>(p->N, p->C, adj, a, batch, nsteps, t0, t1, st);
+  return cuda_status(e);
+}
+
+size_t lf_fft_workspace_bytes(lf_plan_t p, int batch) {
+  if (!p || batch < 0) return 0;
+  return sizeof(double2) * (size_t)batch * p->N * (p->N / 2);
+}
+
+int lf_rfft2(lf_plan_t p, const void* maps, int in_dtype, int batch, void* spec, void* stream) {
+  if (!p) return LF_ERR_BAD_ARG;
+  if (batch < 0) return LF_ERR_BAD_SHAPE;
+  if (in_dtype != LF_F32 && in_dtype != LF_F64) return LF_ERR_BAD_DTYPE;
+  if (batch == 0) return LF_OK;
+  if (!maps || !spec || !aligned16(maps) || !aligned16(spec)) return LF_ERR_BAD_ARG;
+  g_prof = &p->prof;
+  return cuda_status(run_rfft2(p->N, maps, in_dtype == LF_F64, batch, reinterpret_cast<double2*>(spec), p->tw64,
+                               (cudaStream_t)stream));
+}
+
+int lf_irfft2(lf_plan_t p, const void* spec, int batch, void* maps, int out_dtype, void* ws, size_t ws_bytes,
+              void* stream) {
+  if (!p) return LF_ERR_BAD_ARG;
+  if (batch < 0) return LF_ERR_BAD_SHAPE;
+  if (out_dtype != LF_F32 && out_dtype != LF_F64) return LF_ERR_BAD_DTYPE;
+  if (batch == 0) return LF_OK;
+  if (!maps || !spec || !ws || !aligned16(maps) || !aligned16(spec) || !aligned16(ws)) return LF_ERR_BAD_ARG;
+  if (ws_bytes < lf_fft_workspace_bytes(p, batch)) return LF_ERR_WORKSPACE;
+  g_prof = &p->prof;
+  return cuda_status(run_irfft2(p->N, reinterpret_cast<const double2*>(spec), batch, maps, out_dtype == LF_F64,
+                                reinterpret_cast<double2*>(ws), p->tw64, (cudaStream_t)stream));
+}
+
+size_t lf_vjp_workspace_bytes(lf_plan_t p, int batch) {
+  if (!p || batch < 0) return 0;
+  return VjpLayout(p->N, p->C, batch, p->prec == LF_F64 ? 8 : 4).total;
+}
+
+int lf_lense_flow_vjp(lf_plan_t p, const void* f_lensed, const void* cotangent, int io_dtype, const void* planes,
+                      int batch, int nsteps, int direction, void* delta_f, void* f_back, void* dphi, int dphi_basis,
+                      void* ws, size_t ws_bytes, void* stream) {
+  if (!p) return LF_ERR_BAD_ARG;
+  if (batch < 0) return LF_ERR_BAD_SHAPE;
+  if (io_dtype != LF_F32 && io_dtype != LF_F64) return LF_ERR_BAD_DTYPE;
+  if (nsteps < 1 || (direction != LF_FORWARD_LENSE && direction != LF_INVERSE_LENSE)) return LF_ERR_BAD_ARG;
+  if (dphi_basis != LF_PHI_MAP && dphi_basis != LF_PHI_FOURIER) return LF_ERR_BAD_ARG;
+  if (batch == 0) return LF_OK;
+  if (!f_lensed || !cotangent || !planes || !delta_f || !dphi || !ws) return LF_ERR_BAD_ARG;
+  if (!aligned16(f_lensed) || !aligned16(cotangent) || !aligned16(planes) || !aligned16(delta_f) ||
+      !aligned16(dphi) || !aligned16(ws) || (f_back && !aligned16(f_back)))
+    return LF_ERR_BAD_ARG;
+  const size_t el = p->prec == LF_F64 ? 8 : 4;
+  const VjpLayout L(p->N, p->C, batch, el);
+  if (ws_bytes < L.total) return LF_ERR_WORKSPACE;
+  // lense_flow.py:30 integrates in the opposite direction; :54-74 maps it to the time span
+  const int back = -direction;
+  const double t0 = back == LF_INVERSE_LENSE ? 1.0 : 0.0, t1 = back == LF_INVERSE_LENSE ? 0.0 : 1.0;
+  char* w = reinterpret_cast<char*>(ws);
+  const size_t plane = el * (size_t)batch * p->C * p->N * p->N;
+  char* fs = w;
+  char* ds = fs + L.f_sys;
+  char* grad = ds + L.d_sys;
+  char* dsave = grad + L.grad;
+  char* fback = dsave + L.dsave;
+  double* dacc = reinterpret_cast<double*>(fback + L.fback);
+  double2* spec = reinterpret_cast<double2*>(reinterpret_cast<char*>(dacc) + L.dacc);
+  double2* dphi_f = reinterpret_cast<double2*>(reinterpret_cast<char*>(spec) + L.spec);
+  StageArgs af, ad;
+  std::memset(&af, 0, sizeof(af));
+  af.f_in = f_lensed;
+  af.f_out = f_back ? f_back : (void*)fback;
+  af.in_f64 = af.out_f64 = io_dtype == LF_F64;
+  af.phi = planes;
+  af.y0 = fs;
+  af.acc = fs + plane;
+  af.s = fs + 2 * plane;
+  af.gx = fs + 3 * plane;
+  af.twN = p->tw;
+  af.kbase = 2.0 * M_PI / ((double)p->N * p->pix_width);
+  af.nplanes = batch * p->C;
+  af.grad = grad;
+  ad = af;
+  ad.f_in = cotangent;
+  ad.f_out = delta_f;
+  ad.y0 = ds;
+  ad.acc = ds + plane;
+  ad.s = ds + 2 * plane;
+  ad.v = ds + 3 * plane;
+  ad.gx = ds + 4 * plane;
+  ad.grad = nullptr;
+  ad.dsave = dsave;
+  cudaStream_t st = (cudaStream_t)stream;
+  g_prof = &p->prof;
+  cudaError_t e = p->prec == LF_F64 ? run_vjp<double>(p->N, p->C, af, ad, dacc, batch, nsteps, t0, t1, st)
+                                    : run_vjp<float>(p->N, p->C, af, ad, dacc, batch, nsteps, t0, t1, st);
+  if (e != cudaSuccess) return cuda_status(e);
+  // delta-phi = sum_j m_j rfft2(acc_j): rfft2 of the 5B accumulator planes, then combine
+  e = run_rfft2(p->N, dacc, 1, batch * 5, spec, p->tw64, st);
+  if (e != cudaSuccess) return cuda_status(e);
+  const long half = (long)batch * p->N * (p->N / 2 + 1);
+  double2* target = dphi_basis == LF_PHI_FOURIER ? reinterpret_cast<double2*>(dphi) : dphi_f;
+  e = launch<k_dphi_combine>(dim3((unsigned)std::min<long>((half + 255) / 256, 4096)), 256, 0, st,
+                             (const double2*)spec, target, batch, p->N, af.kbase);
+  if (e != cudaSuccess) return cuda_status(e);
+  if (dphi_basis == LF_PHI_MAP)  // the map-basis reference sums irfft2 of each term (lense_flow.py:240-248)
+    e = run_irfft2(p->N, dphi_f, batch, dphi, 1, spec, p->tw64, st);
   return cuda_status(e);
 }
 

@@ -45,6 +45,9 @@ struct StageArgs {
   int stage;        // 1..4 (0 = init)
   int last;         // final stage of the integration
   int nplanes;      // B*C (column pass)
+  // reverse-mode (VJP) extras
+  void* grad;       // standard pass with SAVE: d_x y_s, d_y y_s, [B*C][2][N][N] T
+  void* dsave;      // adjoint pass with SAVE: next stage input, [B*C][N][N] T
 };
 
 // p = M(t)^-1 grad(phi) with M = I + t grad grad phi (lense_flow.py:373-381, :398-415)
@@ -122,7 +125,9 @@ __global__ void __launch_bounds__(NT) k_col(StageArgs a) {
 // the next stage input; stage 4 forms y0 + h/6 (acc + k4).
 // STAGE0 = true: initialisation (copy the input field, transform the first
 // stage input), no rate evaluation.
-template <typename T, int N, int C, bool ADJ, bool STAGE0, int LINES, int NT>
+// SAVE (reverse mode): the standard pass also stores d_x y_s and d_y y_s;
+// the adjoint pass stores its next stage input (the init pass its input).
+template <typename T, int N, int C, bool ADJ, bool STAGE0, int LINES, int NT, bool SAVE = false>
 __global__ void __launch_bounds__(NT) k_row(StageArgs a) {
   constexpr int H = N / 2;
   constexpr long P = (long)N * N;
@@ -209,6 +214,11 @@ __global__ void __launch_bounds__(NT) k_row(StageArgs a) {
           k.x = px * g0.x + py * g1.x;
           p_vector<T>(fx.y, fy.y, fxx.y, fxy.y, fyy.y, tcur, px, py);
           k.y = px * g0.y + py * g1.y;
+          if constexpr (SAVE) {
+            c2<T>* gs = reinterpret_cast<c2<T>*>(reinterpret_cast<T*>(a.grad) + plane * 2 * P + (long)r0 * N);
+            gs[e] = g0;
+            gs[P / 2 + e] = g1;
+          }
         }
         const c2<T> y0 = y0g[e];
         if (a.stage == 1) {
@@ -233,6 +243,9 @@ __global__ void __launch_bounds__(NT) k_row(StageArgs a) {
             y0g[e] = ynext;
           }
         }
+      }
+      if constexpr (SAVE && ADJ) {
+        if (STAGE0 || !a.last) reinterpret_cast<c2<T>*>(reinterpret_cast<T*>(a.dsave) + prow)[e] = ynext;
       }
       if (STAGE0 || !a.last) {
         if constexpr (ADJ) {
@@ -265,8 +278,8 @@ __global__ void __launch_bounds__(NT) k_row(StageArgs a) {
 // ================================================ phi precompute (FP64)
 // rfft along rows of a real map (N x N double) into the unpacked
 // (N x (N/2+1)) complex layout of rfft2.   grid: x = row tile, y = map.
-template <int N, int LINES, int NT>
-__global__ void __launch_bounds__(NT) k_phi_rows_r2c(const double* __restrict__ phi, double2* __restrict__ out,
+template <int N, int LINES, int NT, typename TI = double>
+__global__ void __launch_bounds__(NT) k_phi_rows_r2c(const TI* __restrict__ phi, double2* __restrict__ out,
                                                       const double2* __restrict__ twN) {
   constexpr int H = N / 2;
   extern __shared__ __align__(16) unsigned char smem_raw[];
@@ -276,8 +289,8 @@ __global__ void __launch_bounds__(NT) k_phi_rows_r2c(const double* __restrict__ 
   const int r0 = blockIdx.x * LINES;
   const long map = blockIdx.y;
   load_twiddles<double, N, NT>(tw, twN, tid);
-  const double2* src = reinterpret_cast<const double2*>(phi + map * (long)N * N + (long)r0 * N);
-  load_rows<double, double2, H, LINES, NT>(buf, src, H, tid);
+  const c2<TI>* src = reinterpret_cast<const c2<TI>*>(phi + map * (long)N * N + (long)r0 * N);
+  load_rows<double, c2<TI>, H, LINES, NT>(buf, src, H, tid);
   __syncthreads();
   fft_tiles<double, H, LINES, 1, NT, false, N>(buf, tw, tid);
   r2c_post<double, H, LINES, 1, NT>(buf, tw, tid);
@@ -411,6 +424,102 @@ __global__ void k_min_det(const T* __restrict__ planes, long P, int* __restrict_
   }
   for (int o = 16; o > 0; o >>= 1) best = fmin(best, __shfl_xor_sync(0xffffffffu, best, o));
   if ((threadIdx.x & 31) == 0) atomicMin(out + map, ordered_int(float(best)));
+}
+
+// ======================================================= reverse mode
+// delta-phi accumulation for one RK4 stage (lense_flow.py:195-252).  With
+// fdf = sum_c df_c grad f_c, a = M^-1 fdf, w = p (x) a, the stage rate is
+//   D_x a_x + D_y a_y + t (D_xx w_xx + D_xy (w_xy + w_yx) + D_yy w_yy).
+// delta-phi never feeds back into the ODE, so its RK4 sum is linear in the
+// rates: the five pre-derivative fields are accumulated with the stage
+// weight h/6 {1,2,2,1} here and the derivative multipliers are applied once
+// at the end (k_dphi_combine).  Accumulators are float64, [B][5][N][N].
+template <typename T, int C>
+__global__ void k_dphi_accum(const T* __restrict__ grad, const T* __restrict__ dsave, const T* __restrict__ phi,
+                             double* __restrict__ acc, int B, long P, double t, double wgt, int first) {
+  const long total = (long)B * P;
+  for (long i = blockIdx.x * (long)blockDim.x + threadIdx.x; i < total; i += (long)gridDim.x * blockDim.x) {
+    const long b = i / P, px = i % P;
+    double fx = 0.0, fy = 0.0;
+#pragma unroll
+    for (int c = 0; c < C; ++c) {
+      const long pl = b * C + c;
+      const double d = dsave[pl * P + px];
+      fx += d * double(grad[pl * 2 * P + px]);
+      fy += d * double(grad[pl * 2 * P + P + px]);
+    }
+    const T* ph = phi + b * 5 * P + px;
+    const double gx = ph[0], gy = ph[P], gxx = ph[2 * P], gxy = ph[3 * P], gyy = ph[4 * P];
+    const double mxx = 1.0 + t * gxx, mxy = t * gxy, myy = 1.0 + t * gyy;
+    const double inv = 1.0 / (mxx * myy - mxy * mxy + 1e-12);
+    const double ixx = myy * inv, ixy = -mxy * inv, iyy = mxx * inv;
+    const double ax = ixx * fx + ixy * fy, ay = ixy * fx + iyy * fy;
+    const double pxv = gx * ixx + gy * ixy, pyv = gx * ixy + gy * iyy;
+    const double v[5] = {ax, ay, t * pxv * ax, t * (pxv * ay + pyv * ax), t * pyv * ay};
+    double* o = acc + b * 5 * P + px;
+#pragma unroll
+    for (int j = 0; j < 5; ++j) o[j * P] = first ? wgt * v[j] : o[j * P] + wgt * v[j];
+  }
+}
+
+// delta-phi in the rfft2 layout: sum_j m_j * rfft2(acc_j) with the raw
+// multipliers of get_primal_derivatives_to_fourier (util.py:133-137):
+// i KX, i KY, -KX^2, -KX KY, -KY^2 (KY's Nyquist entry negated).
+// ``spec`` holds rfft2(acc_j) as [B][5][N][N/2+1].
+__global__ void k_dphi_combine(const double2* __restrict__ spec, double2* __restrict__ out, int B, int N,
+                               double kbase) {
+  const int H = N / 2;
+  const long per = (long)N * (H + 1);
+  const long total = (long)B * per;
+  for (long i = blockIdx.x * (long)blockDim.x + threadIdx.x; i < total; i += (long)gridDim.x * blockDim.x) {
+    const long b = i / per, r = i % per;
+    const int k0 = (int)(r / (H + 1)), k1 = (int)(r % (H + 1));
+    const double kx = kbase * double(k0 < N / 2 ? k0 : k0 - N);
+    const double ky = (k1 == H) ? -kbase * double(H) : kbase * double(k1);
+    const double2* s = spec + b * 5 * per + r;
+    const double2 s0 = s[0], s1 = s[per], s2 = s[2 * per], s3 = s[3 * per], s4 = s[4 * per];
+    double re = -kx * s0.y - ky * s1.y;
+    double im = kx * s0.x + ky * s1.x;
+    const double q2 = -kx * kx, q3 = -kx * ky, q4 = -ky * ky;
+    re += q2 * s2.x + q3 * s3.x + q4 * s4.x;
+    im += q2 * s2.y + q3 * s3.y + q4 * s4.y;
+    out[i] = make_double2(re, im);
+  }
+}
+
+// Inverse column FFT of an unpacked (N x (N/2+1)) spectrum, scaled by
+// 1/N^2, into packed rows whose slot 0 keeps the real parts of columns 0 and
+// N/2 (what irfft2 keeps).  grid: x = column tile, y = map.
+template <int N, int LINES, int NT>
+__global__ void __launch_bounds__(NT) k_spec_cols_inv(const double2* __restrict__ spec, double2* __restrict__ packed,
+                                                       const double2* __restrict__ twN) {
+  constexpr int H = N / 2;
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  double2* tw = reinterpret_cast<double2*>(smem_raw);
+  double2* buf = tw + N;
+  const int tid = threadIdx.x;
+  const int c0 = blockIdx.x * LINES;
+  const long map = blockIdx.y;
+  load_twiddles<double, N, NT>(tw, twN, tid);
+  load_cols<double, N, LINES, NT>(buf, spec + map * (long)N * (H + 1), H + 1, c0, H + 1, tid);
+  __syncthreads();
+  const double scale = 1.0 / (double(N) * double(N));
+  for (int idx = tid; idx < N * LINES; idx += NT) {
+    const int m = idx / LINES, line = idx % LINES;
+    const double2 v = buf[sw<LINES>(m, line)];
+    buf[sw<LINES>(m, line)] = make_double2(v.x * scale, v.y * scale);
+  }
+  __syncthreads();
+  fft_tiles<double, N, LINES, 1, NT, true, N>(buf, tw, tid);
+  double2* out = packed + map * (long)N * H;
+  for (int idx = tid; idx < N * LINES; idx += NT) {
+    const int m = idx / LINES, line = idx % LINES;
+    const int col = c0 + line;
+    const double2 v = buf[sw<LINES>(m, line)];
+    if (col == 0) reinterpret_cast<double*>(out + (long)m * H)[0] = v.x;
+    else if (col == H) reinterpret_cast<double*>(out + (long)m * H)[1] = v.x;
+    else if (col < H) out[(long)m * H + col] = v;
+  }
 }
 
 }  // namespace lf

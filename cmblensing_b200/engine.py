@@ -132,6 +132,74 @@ class Plan:
         return out
 
 
+    # ------------------------------------------------------------ FFTs
+    def rfft2(self, maps):
+        """float64 rfft2 of [B,N,N] float32/float64 maps -> [B,N,N/2+1] complex128 (jnp.fft.rfft2)."""
+        N = self.nside
+        maps = maps.contiguous()
+        if maps.dim() == 2:
+            maps = maps.unsqueeze(0)
+        if maps.shape[-2:] != (N, N) or maps.dtype not in (torch.float32, torch.float64):
+            raise nat.LenseFlowError(nat.LF_ERR_BAD_SHAPE, f"maps {tuple(maps.shape)} {maps.dtype}")
+        B = maps.shape[0]
+        spec = torch.empty((B, N, N // 2 + 1), dtype=torch.complex128, device=self.device)
+        code = nat.LF_F64 if maps.dtype == torch.float64 else nat.LF_F32
+        with torch.cuda.device(self.device):
+            nat.check(self._lib.lf_rfft2(self.handle, _ptr(maps), code, B, _ptr(spec), _stream_ptr(self.device)),
+                      "lf_rfft2")
+        return spec
+
+    def irfft2(self, spec, out_dtype=torch.float64):
+        """float64 irfft2 of [B,N,N/2+1] complex128 -> [B,N,N] maps (jnp.fft.irfft2 semantics)."""
+        N = self.nside
+        spec = spec.to(torch.complex128).contiguous()
+        if spec.dim() == 2:
+            spec = spec.unsqueeze(0)
+        if spec.shape[-2:] != (N, N // 2 + 1):
+            raise nat.LenseFlowError(nat.LF_ERR_BAD_SHAPE, f"spectrum {tuple(spec.shape)}")
+        B = spec.shape[0]
+        maps = torch.empty((B, N, N), dtype=out_dtype, device=self.device)
+        ws = torch.empty(max(int(self._lib.lf_fft_workspace_bytes(self.handle, B)), 16), dtype=torch.uint8,
+                         device=self.device)
+        code = nat.LF_F64 if out_dtype == torch.float64 else nat.LF_F32
+        with torch.cuda.device(self.device):
+            nat.check(self._lib.lf_irfft2(self.handle, _ptr(spec), B, _ptr(maps), code, _ptr(ws), ws.numel(),
+                                          _stream_ptr(self.device)), "lf_irfft2")
+        return maps
+
+    # ------------------------------------------------------------ VJP
+    def lense_flow_vjp(self, f_lensed, cotangent, planes, n=10, direction=FORWARD_LENSE, phi_basis="fourier",
+                       return_f=False):
+        """The reference's reverse pass (lense_flow.py:23-126) for [B,C,N,N] fields.
+
+        Returns (delta_f, delta_phi[, f_back]) with delta_f before undo_inner_product and
+        delta_phi [B,N,N/2+1] complex128 (phi_basis "fourier") or [B,N,N] float64 ("map").
+        """
+        N, C = self.nside, self.ncomp
+        if f_lensed.shape != cotangent.shape or f_lensed.dim() != 4 or f_lensed.shape[1:] != (C, N, N):
+            raise nat.LenseFlowError(nat.LF_ERR_BAD_SHAPE, "field/cotangent shapes")
+        dt = torch.float64 if torch.float64 in (f_lensed.dtype, cotangent.dtype) else torch.float32
+        fl = f_lensed.to(dt).contiguous()
+        ct = cotangent.to(dt).contiguous()
+        B = fl.shape[0]
+        if planes.shape != (B, 5, N, N) or planes.dtype != self.dtype:
+            raise nat.LenseFlowError(nat.LF_ERR_BAD_SHAPE, "phi planes do not match")
+        df = torch.empty_like(fl)
+        fb = torch.empty_like(fl) if return_f else None
+        fourier = phi_basis == "fourier"
+        dphi = (torch.empty((B, N, N // 2 + 1), dtype=torch.complex128, device=self.device) if fourier
+                else torch.empty((B, N, N), dtype=torch.float64, device=self.device))
+        ws = torch.empty(max(int(self._lib.lf_vjp_workspace_bytes(self.handle, B)), 16), dtype=torch.uint8,
+                         device=self.device)
+        code = nat.LF_F64 if dt == torch.float64 else nat.LF_F32
+        with torch.cuda.device(self.device):
+            nat.check(self._lib.lf_lense_flow_vjp(self.handle, _ptr(fl), _ptr(ct), code, _ptr(planes), B, int(n),
+                                                  int(direction), _ptr(df), _ptr(fb) if fb is not None else None,
+                                                  _ptr(dphi), nat.LF_PHI_FOURIER if fourier else nat.LF_PHI_MAP,
+                                                  _ptr(ws), ws.numel(), _stream_ptr(self.device)),
+                      "lf_lense_flow_vjp")
+        return (df, dphi, fb) if return_f else (df, dphi)
+
     # ---------------------------------------------------------- profiling
     def profile(self, enable=True):
         nat.check(self._lib.lf_profile_enable(self.handle, int(bool(enable))), "lf_profile_enable")
@@ -185,6 +253,50 @@ class HostPipeline:
         return out_host
 
 
+class LenseFlowFunction(torch.autograd.Function):
+    """torch autograd for y = L(phi) f on device tensors.
+
+    f: [B,C,N,N]; phi: [B,N,N] real map or [B,N,N/2+1] complex Fourier.
+    The backward pass is the reference's scheme (lense_flow.py:23-126): the
+    f-cotangent is the exact adjoint lens of the incoming gradient, the
+    phi-cotangent the continuous adjoint integrated with RK4 (it matches the
+    exact discrete gradient to the RK4 discretisation error).  For a complex
+    Fourier phi the gradient follows torch's convention dL/dRe + i dL/dIm,
+    i.e. the reference's delta-phi times w/N^2 (w = 1 on the DC/Nyquist
+    columns, 2 elsewhere).
+    """
+
+    @staticmethod
+    def forward(ctx, f, phi, pix_width, n, direction, precision):
+        plan = get_plan(f.shape[-1], f.shape[1], pix_width, precision, device=f.device)
+        planes = plan.phi_planes(phi.detach(), check_det=False)
+        out = plan.lense_flow(f.detach(), planes, n=n, direction=direction)
+        ctx.save_for_backward(out, planes)
+        ctx.plan, ctx.n, ctx.direction = plan, n, direction
+        ctx.fourier = phi.is_complex()
+        ctx.phi_dtype, ctx.f_dtype = phi.dtype, f.dtype
+        return out
+
+    @staticmethod
+    def backward(ctx, g):
+        out, planes = ctx.saved_tensors
+        plan = ctx.plan
+        df, dphi = plan.lense_flow_vjp(out, g.contiguous(), planes, n=ctx.n, direction=ctx.direction,
+                                       phi_basis="fourier" if ctx.fourier else "map")
+        if ctx.fourier:
+            N = plan.nside
+            w = torch.full((N // 2 + 1,), 2.0, dtype=torch.float64, device=dphi.device)
+            w[0] = 1.0
+            w[-1] = 1.0
+            dphi = dphi * (w / (N * N))
+        return df.to(ctx.f_dtype), dphi.to(ctx.phi_dtype), None, None, None, None
+
+
+def lense_flow_ad(f, phi, pix_width, n=10, direction=FORWARD_LENSE, precision="f32"):
+    """Differentiable LenseFlow (torch autograd) on device tensors."""
+    return LenseFlowFunction.apply(f, phi, pix_width, n, direction, precision)
+
+
 def get_plan(nside, ncomp, pix_width, precision="f32", device=None):
     dev = torch.cuda.current_device() if device is None else torch.device(device).index
     key = (dev, int(nside), int(ncomp), float(pix_width), precision)
@@ -206,4 +318,5 @@ def lense_flow_batch(f, phi, pix_width, n=10, direction=FORWARD_LENSE, adjoint=F
     return plan.lense_flow(f, planes, n=n, direction=direction, adjoint=adjoint)
 
 
-__all__ = ["Plan", "HostPipeline", "get_plan", "lense_flow_batch", "FORWARD_LENSE", "INVERSE_LENSE"]
+__all__ = ["Plan", "HostPipeline", "LenseFlowFunction", "get_plan", "lense_flow_ad", "lense_flow_batch",
+           "FORWARD_LENSE", "INVERSE_LENSE"]

@@ -89,6 +89,33 @@ int lf_lense_flow(lf_plan_t plan, const void* f_in, int in_dtype, void* f_out, i
                   int batch, int nsteps, int direction, int adjoint, void* workspace, size_t workspace_bytes,
                   void* stream);
 
+/* float64 2-D real FFTs in the reference's layout (util.py:113, fields.py:159-172):
+ * lf_rfft2: maps [batch][N][N] (float32/float64) -> spec [batch][N][N/2+1]
+ * complex128, unnormalised (jnp.fft.rfft2).  lf_irfft2: spec -> maps,
+ * 1/N^2 normalised, imaginary parts of the DC/Nyquist columns ignored after
+ * the column transform (jnp.fft.irfft2).  lf_irfft2 needs
+ * lf_fft_workspace_bytes of scratch.  Replace the rfft2/irfft2 calls of
+ * fields.py:159-172 (map, fourier) and fields.py:147-154 (undo_inner_product). */
+size_t lf_fft_workspace_bytes(lf_plan_t plan, int batch);
+int lf_rfft2(lf_plan_t plan, const void* maps, int in_dtype, int batch, void* spec, void* stream);
+int lf_irfft2(lf_plan_t plan, const void* spec, int batch, void* maps, int out_dtype, void* workspace,
+              size_t workspace_bytes, void* stream);
+
+/* Reverse-mode derivative of lf_lense_flow in the reference's scheme
+ * (lense_flow_backwards / get_lensing_operator_gradients /
+ * lensing_gradients_integration_step / get_delta_phi_tqu_roc,
+ * cmb_lensing/lense_flow.py:23-126, :156-252): from the lensed field
+ * ``f_lensed`` and the cotangent, integrate (f, delta_f, delta_phi) with RK4
+ * in the opposite time direction.  Outputs: ``delta_f`` [batch][ncomp][N][N]
+ * (before undo_inner_product), optional ``f_back`` (the re-integrated field),
+ * and ``dphi``: [batch][N][N/2+1] complex128 if dphi_basis = LF_PHI_FOURIER
+ * (accumulated in Fourier space, lense_flow.py:233-239) or [batch][N][N]
+ * float64 if LF_PHI_MAP (lense_flow.py:240-248). */
+size_t lf_vjp_workspace_bytes(lf_plan_t plan, int batch);
+int lf_lense_flow_vjp(lf_plan_t plan, const void* f_lensed, const void* cotangent, int io_dtype, const void* planes,
+                      int batch, int nsteps, int direction, void* delta_f, void* f_back, void* dphi, int dphi_basis,
+                      void* workspace, size_t workspace_bytes, void* stream);
+
 /* Launch timing for benchmarks and profiling.  While enabled, every kernel
  * launched through ``plan`` is bracketed by a CUDA event pair on its stream.
  * lf_profile_read synchronises on the last event and returns the summed
