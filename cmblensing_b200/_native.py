@@ -47,10 +47,13 @@ SIGNATURES = {
     "lf_irfft2": (_i, [_vp, _vp, _i, _vp, _i, _vp, _sz, _vp]),
     "lf_vjp_workspace_bytes": (_sz, [_vp, _i]),
     "lf_lense_flow_vjp": (_i, [_vp, _vp, _vp, _i, _vp, _i, _i, _i, _vp, _vp, _vp, _i, _vp, _sz, _vp]),
+    "lf_lense_flow_noalloc": (_i, [_i, _i, ctypes.c_double, _vp, _i, _vp, _i, _vp, _i, _i, _i, _i, _vp]),
     "lf_profile_enable": (_i, [_vp, _i]),
     "lf_profile_reset": (_i, [_vp]),
     "lf_profile_read": (_i, [_vp, _i, ctypes.POINTER(ctypes.c_double), ctypes.POINTER(_i)]),
 }
+
+LF_NOALLOC_SCRATCH_BYTES = 24 * 1024 * 1024
 
 LF_KIND_ROW = 0
 LF_KIND_COL = 1

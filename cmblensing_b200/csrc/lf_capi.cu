@@ -5,6 +5,7 @@
 #include <algorithm>
 #include <cmath>
 #include <cstring>
+#include <mutex>
 #include <new>
 #include <vector>
 
@@ -663,3 +664,109 @@ int lf_profile_read(lf_plan_t p, int kind, double* total_ms, int* launches) {
 }
 
 }  // extern "C"
+
+// ------------------------------------------------ allocation-free entry point
+// lf_lense_flow_noalloc keeps its scratch in file-scope device arrays instead
+// of caller- or library-allocated memory.  In host code these symbols are
+// host-side stand-ins, not device addresses: their device addresses come
+// from cudaGetSymbolAddress, taken once per device (with that device current)
+// on the first call on the device, and only those addresses reach kernels.
+static __device__ __align__(256) unsigned char g_noalloc_scratch[LF_NOALLOC_SCRATCH_BYTES];
+static __device__ __align__(256) float2 g_noalloc_tw[64 + 128 + 256 + 512 + 1024];
+
+namespace {
+
+struct NoAllocDevice {
+  bool ready = false;
+  char* scratch = nullptr;  // device address of g_noalloc_scratch
+  float2* tw = nullptr;     // device address of g_noalloc_tw
+};
+
+constexpr int kNoAllocMaxDevices = 64;
+NoAllocDevice g_noalloc_dev[kNoAllocMaxDevices];
+std::mutex g_noalloc_mu;
+
+int noalloc_tw_offset(int n) {
+  return n == 64 ? 0 : n == 128 ? 64 : n == 256 ? 192 : n == 512 ? 448 : 960;
+}
+
+// Once per device: resolve the arrays' device addresses and fill the twiddle
+// tables (exp(-2 pi i k / N), float64 on the host, rounded once) with a
+// synchronous copy.  No device or host heap allocation.
+int noalloc_setup(NoAllocDevice** out) {
+  int dev = 0;
+  cudaError_t e = cudaGetDevice(&dev);
+  if (e != cudaSuccess) return cuda_status(e);
+  if (dev < 0 || dev >= kNoAllocMaxDevices) return LF_ERR_CUDA;
+  std::lock_guard<std::mutex> lock(g_noalloc_mu);
+  NoAllocDevice& d = g_noalloc_dev[dev];
+  if (!d.ready) {
+    void* scratch = nullptr;
+    void* tw = nullptr;
+    e = cudaGetSymbolAddress(&scratch, g_noalloc_scratch);
+    if (e != cudaSuccess) return cuda_status(e);
+    e = cudaGetSymbolAddress(&tw, g_noalloc_tw);
+    if (e != cudaSuccess) return cuda_status(e);
+    static float2 host[64 + 128 + 256 + 512 + 1024];
+    for (int n = 64; n <= 1024; n *= 2) {
+      const int off = noalloc_tw_offset(n);
+      for (int k = 0; k < n; ++k) {
+        const double ang = -2.0 * M_PI * (double)k / (double)n;
+        host[off + k] = make_float2((float)std::cos(ang), (float)std::sin(ang));
+      }
+    }
+    e = cudaMemcpyToSymbol(g_noalloc_tw, host, sizeof(host));
+    if (e != cudaSuccess) return cuda_status(e);
+    d.scratch = reinterpret_cast<char*>(scratch);
+    d.tw = reinterpret_cast<float2*>(tw);
+    d.ready = true;
+  }
+  *out = &d;
+  return LF_OK;
+}
+
+}  // namespace
+
+extern "C" int lf_lense_flow_noalloc(int nside, int ncomp, double pix_width, const void* f_in, int in_dtype,
+                                     void* f_out, int out_dtype, const void* planes, int batch, int nsteps,
+                                     int direction, int adjoint, void* stream) {
+  if (!valid_n(nside) || ncomp < 1 || ncomp > 3 || batch < 0) return LF_ERR_BAD_SHAPE;
+  if ((in_dtype != LF_F32 && in_dtype != LF_F64) || (out_dtype != LF_F32 && out_dtype != LF_F64))
+    return LF_ERR_BAD_DTYPE;
+  if (!(pix_width > 0.0) || !std::isfinite(pix_width)) return LF_ERR_BAD_ARG;
+  if (nsteps < 0 || (direction != LF_FORWARD_LENSE && direction != LF_INVERSE_LENSE)) return LF_ERR_BAD_ARG;
+  const bool adj = adjoint != 0;
+  const size_t npix = (size_t)nside * nside * (size_t)batch * ncomp;
+  const size_t plane_bytes = 4 * npix;  // float32 compute
+  if (plane_bytes * (adj ? 5 : 4) > (size_t)LF_NOALLOC_SCRATCH_BYTES) return LF_ERR_WORKSPACE;
+  if (batch == 0) return LF_OK;
+  if (!f_in || !f_out || !planes || !aligned16(f_in) || !aligned16(f_out) || !aligned16(planes)) return LF_ERR_BAD_ARG;
+  cudaStream_t st = (cudaStream_t)stream;
+  if (nsteps == 0) {
+    if (in_dtype != out_dtype) return LF_ERR_BAD_DTYPE;
+    if (f_in == f_out) return LF_OK;
+    return cuda_status(cudaMemcpyAsync(f_out, f_in, npix * (in_dtype == LF_F64 ? 8 : 4), cudaMemcpyDeviceToDevice, st));
+  }
+  NoAllocDevice* d = nullptr;
+  const int s = noalloc_setup(&d);
+  if (s != LF_OK) return s;
+  const bool fwd_time = ((direction == LF_FORWARD_LENSE) != adj);
+  const double t0 = fwd_time ? 0.0 : 1.0, t1 = fwd_time ? 1.0 : 0.0;
+  StageArgs a;
+  std::memset(&a, 0, sizeof(a));
+  a.f_in = f_in;
+  a.f_out = f_out;
+  a.in_f64 = in_dtype == LF_F64;
+  a.out_f64 = out_dtype == LF_F64;
+  a.phi = planes;
+  a.y0 = d->scratch;
+  a.acc = d->scratch + plane_bytes;
+  a.s = d->scratch + 2 * plane_bytes;
+  a.gx = d->scratch + 3 * plane_bytes;
+  a.v = adj ? (void*)(d->scratch + 4 * plane_bytes) : nullptr;
+  a.twN = d->tw + noalloc_tw_offset(nside);
+  a.kbase = 2.0 * M_PI / ((double)nside * pix_width);
+  a.nplanes = batch * ncomp;
+  g_prof = nullptr;
+  return cuda_status(run_lens<float>(nside, ncomp, adj, a, batch, nsteps, t0, t1, st));
+}

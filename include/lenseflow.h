@@ -116,6 +116,27 @@ int lf_lense_flow_vjp(lf_plan_t plan, const void* f_lensed, const void* cotangen
                       int batch, int nsteps, int direction, void* delta_f, void* f_back, void* dphi, int dphi_basis,
                       void* workspace, size_t workspace_bytes, void* stream);
 
+/* Allocation-free variant of lf_lense_flow (float32 compute), for callers
+ * that cannot allocate device memory: a host framework that has already
+ * reserved (nearly) all of the GPU's memory for its own pool, where one more
+ * cudaMalloc can fail, and latency-critical loops where cudaMalloc/cudaFree
+ * would synchronise the device.  No counterpart in the reference.
+ * The caller passes the inputs (fields, derivative planes from
+ * lf_phi_precompute) and the output; there is no plan: the geometry is
+ * passed directly.  Scratch lives in a file-scope device array of
+ * LF_NOALLOC_SCRATCH_BYTES that every GPU which loads the library holds until
+ * exit; a call needing more (4 bytes x N^2 x batch x ncomp x (4, or 5 when
+ * adjoint)) returns LF_ERR_WORKSPACE.  The first call on each device resolves
+ * the array's device address and fills twiddle tables with a synchronous
+ * copy: make that first call before any stream capture.  Every call shares
+ * the one array, so calls that overlap on the GPU (other streams, other host
+ * threads) race; serialise them.  No scratch element needs to start at zero:
+ * each is written before it is read within a call. */
+#define LF_NOALLOC_SCRATCH_BYTES (24u * 1024u * 1024u)
+int lf_lense_flow_noalloc(int nside, int ncomp, double pix_width, const void* f_in, int in_dtype, void* f_out,
+                          int out_dtype, const void* planes, int batch, int nsteps, int direction, int adjoint,
+                          void* stream);
+
 /* Launch timing for benchmarks and profiling.  While enabled, every kernel
  * launched through ``plan`` is bracketed by a CUDA event pair on its stream.
  * lf_profile_read synchronises on the last event and returns the summed
