@@ -56,13 +56,19 @@ int cuda_status(cudaError_t e) {
 
 // Launch geometry per (precision, N).
 template <typename T> struct Geo;
+// FP32 stage kernels: enough warps per SM to keep ~50 KB of loads in flight;
+// minb() caps registers at 64 per thread so that many blocks fit.
 template <> struct Geo<float> {
-  static constexpr int LINES = 16;
-  static constexpr int nt(int n) { return n <= 64 ? 128 : (n <= 512 ? 256 : 512); }
+  static constexpr int LINES = 16;     // column-pass tile
+  static constexpr int ROW_LINES = 8;  // row-pass tile (all C components at once)
+  static constexpr int nt(int n) { return n <= 64 ? 128 : (n <= 256 ? 256 : (n <= 512 ? 512 : 1024)); }
+  static constexpr int minb(int n) { return 65536 / (nt(n) * 64); }
 };
 template <> struct Geo<double> {
   static constexpr int LINES = 8;
+  static constexpr int ROW_LINES = 4;
   static constexpr int nt(int n) { return n <= 64 ? 64 : (n <= 128 ? 128 : (n <= 512 ? 256 : 512)); }
+  static constexpr int minb(int) { return 1; }
 };
 
 // Opt in to > 48 KB of dynamic shared memory once per kernel and device.
@@ -104,11 +110,13 @@ cudaError_t launch(dim3 grid, int nt, size_t smem, cudaStream_t st, Args... args
 template <typename T, int N, int C, bool ADJ>
 cudaError_t run_lens_n(const StageArgs& base, int B, int nsteps, double t0, double t1, cudaStream_t st) {
   constexpr int LINES = Geo<T>::LINES;
+  constexpr int RL = Geo<T>::ROW_LINES;
   constexpr int NT = Geo<T>::nt(N);
+  constexpr int MB = Geo<T>::minb(N);
   constexpr int H = N / 2;
-  const size_t smem_row = sizeof(c2<T>) * (N + 2 * LINES * H);
+  const size_t smem_row = sizeof(c2<T>) * (N + 2 * C * RL * H);
   const size_t smem_col = sizeof(c2<T>) * (N + LINES * N);
-  const dim3 grow(N / LINES, B);
+  const dim3 grow(N / RL, B);
   const dim3 gcol(H / LINES, B * C);
   StageArgs a = base;
   cudaError_t e;
@@ -119,7 +127,7 @@ cudaError_t run_lens_n(const StageArgs& base, int B, int nsteps, double t0, doub
   a.last = 0;
   a.t_cur = t0;
   a.t_next = t0;
-  e = launch_k<k_row<T, N, C, ADJ, true, LINES, NT>>(LF_KIND_ROW, grow, NT, smem_row, st, a);
+  e = launch_k<k_row<T, N, C, ADJ, true, RL, NT, false, MB>>(LF_KIND_ROW, grow, NT, smem_row, st, a);
   if (e != cudaSuccess) return e;
   for (int i = 0; i < nsteps; ++i) {
     const double t = t0 + i * h;  // util.py:189
@@ -130,9 +138,9 @@ cudaError_t run_lens_n(const StageArgs& base, int B, int nsteps, double t0, doub
       a.t_cur = tc[s];
       a.t_next = tn[s];
       a.last = (i == nsteps - 1 && s == 3);
-      e = launch_k<k_col<T, N, LINES, NT>>(LF_KIND_COL, gcol, NT, smem_col, st, a);
+      e = launch_k<k_col<T, N, LINES, NT, MB>>(LF_KIND_COL, gcol, NT, smem_col, st, a);
       if (e != cudaSuccess) return e;
-      e = launch_k<k_row<T, N, C, ADJ, false, LINES, NT>>(LF_KIND_ROW, grow, NT, smem_row, st, a);
+      e = launch_k<k_row<T, N, C, ADJ, false, RL, NT, false, MB>>(LF_KIND_ROW, grow, NT, smem_row, st, a);
       if (e != cudaSuccess) return e;
     }
   }
@@ -287,11 +295,13 @@ template <typename T, int N, int C>
 cudaError_t run_vjp_n(const StageArgs& af0, const StageArgs& ad0, double* dacc, int B, int nsteps, double t0,
                       double t1, cudaStream_t st) {
   constexpr int LINES = Geo<T>::LINES;
+  constexpr int RL = Geo<T>::ROW_LINES;
   constexpr int NT = Geo<T>::nt(N);
+  constexpr int MB = Geo<T>::minb(N);
   constexpr int H = N / 2;
-  const size_t smem_row = sizeof(c2<T>) * (N + 2 * LINES * H);
+  const size_t smem_row = sizeof(c2<T>) * (N + 2 * C * RL * H);
   const size_t smem_col = sizeof(c2<T>) * (N + LINES * N);
-  const dim3 grow(N / LINES, B);
+  const dim3 grow(N / RL, B);
   const dim3 gcol(H / LINES, B * C);
   const long P = (long)N * N;
   const int gacc = (int)std::min<long>(((long)B * P + 255) / 256, 4096);
@@ -303,9 +313,9 @@ cudaError_t run_vjp_n(const StageArgs& af0, const StageArgs& ad0, double* dacc, 
   af.stage = ad.stage = 0;
   af.last = ad.last = 0;
   af.t_cur = af.t_next = ad.t_cur = ad.t_next = t0;
-  cudaError_t e = launch_k<k_row<T, N, C, false, true, LINES, NT, false>>(LF_KIND_ROW, grow, NT, smem_row, st, af);
+  cudaError_t e = launch_k<k_row<T, N, C, false, true, RL, NT, false, MB>>(LF_KIND_ROW, grow, NT, smem_row, st, af);
   if (e != cudaSuccess) return e;
-  e = launch_k<k_row<T, N, C, true, true, LINES, NT, true>>(LF_KIND_ROW, grow, NT, smem_row, st, ad);
+  e = launch_k<k_row<T, N, C, true, true, RL, NT, true, MB>>(LF_KIND_ROW, grow, NT, smem_row, st, ad);
   if (e != cudaSuccess) return e;
   for (int i = 0; i < nsteps; ++i) {
     const double t = t0 + i * h;
@@ -317,16 +327,16 @@ cudaError_t run_vjp_n(const StageArgs& af0, const StageArgs& ad0, double* dacc, 
       af.t_cur = ad.t_cur = tc[s];
       af.t_next = ad.t_next = tn[s];
       af.last = ad.last = last;
-      e = launch_k<k_col<T, N, LINES, NT>>(LF_KIND_COL, gcol, NT, smem_col, st, af);
+      e = launch_k<k_col<T, N, LINES, NT, MB>>(LF_KIND_COL, gcol, NT, smem_col, st, af);
       if (e != cudaSuccess) return e;
-      e = launch_k<k_row<T, N, C, false, false, LINES, NT, true>>(LF_KIND_ROW, grow, NT, smem_row, st, af);
+      e = launch_k<k_row<T, N, C, false, false, RL, NT, true, MB>>(LF_KIND_ROW, grow, NT, smem_row, st, af);
       if (e != cudaSuccess) return e;
       e = launch<k_dphi_accum<T, C>>(dim3(gacc), 256, 0, st, (const T*)af.grad, (const T*)ad.dsave,
                                      (const T*)af.phi, dacc, B, P, tc[s], h / 6.0 * cw[s], (int)(i == 0 && s == 0));
       if (e != cudaSuccess) return e;
-      e = launch_k<k_col<T, N, LINES, NT>>(LF_KIND_COL, gcol, NT, smem_col, st, ad);
+      e = launch_k<k_col<T, N, LINES, NT, MB>>(LF_KIND_COL, gcol, NT, smem_col, st, ad);
       if (e != cudaSuccess) return e;
-      e = launch_k<k_row<T, N, C, true, false, LINES, NT, true>>(LF_KIND_ROW, grow, NT, smem_row, st, ad);
+      e = launch_k<k_row<T, N, C, true, false, RL, NT, true, MB>>(LF_KIND_ROW, grow, NT, smem_row, st, ad);
       if (e != cudaSuccess) return e;
     }
   }

@@ -24,6 +24,8 @@
 #include <cuda_runtime.h>
 #include <stdint.h>
 
+#include <type_traits>
+
 namespace lf {
 
 template <typename T> struct V2;
@@ -131,8 +133,17 @@ template <int R, typename T, bool INV> __device__ __forceinline__ void dft(c2<T>
 }
 
 // ------------------------------------------------------------ tile layout
-template <int LINES> __device__ __forceinline__ int sw(int m, int line) {
-  return m * LINES + (line ^ (m & (LINES - 1)));
+// The XOR key changes every (128 bytes / (LINES x element size)) rows so
+// that 16 (8-byte elements) or 8 (16-byte elements) consecutive m of one
+// line land in distinct banks: m & 15 for 16 float2 lines, (m >> 1) & 7 for
+// 8 float2 lines, m & 7 for 8 double2 lines.
+template <typename T, int LINES> __device__ __forceinline__ int sw(int m, int line) {
+  constexpr int ROWS_PER_128B = (128 / int(sizeof(c2<T>))) / LINES;
+  if constexpr (ROWS_PER_128B >= 2) {
+    return m * LINES + (line ^ ((m / ROWS_PER_128B) & (LINES - 1)));
+  } else {
+    return m * LINES + (line ^ (m & (LINES - 1)));
+  }
 }
 
 // ------------------------------------------------------------ Stockham pass
@@ -158,7 +169,7 @@ __device__ __forceinline__ void stockham_pass(c2<T>* __restrict__ buf, const c2<
       const int tile = rest / NB;
       const c2<T>* tb = buf + tile * TILE_ELEMS;
 #pragma unroll
-      for (int r = 0; r < R; ++r) v[b][r] = tb[sw<LINES>(j + r * NB, line)];
+      for (int r = 0; r < R; ++r) v[b][r] = tb[sw<T, LINES>(j + r * NB, line)];
       if constexpr (NS > 1) {
         const int k = j % NS;
 #pragma unroll
@@ -180,7 +191,7 @@ __device__ __forceinline__ void stockham_pass(c2<T>* __restrict__ buf, const c2<
       const int k = j % NS;
       const int base = (j / NS) * NS * R + k;
 #pragma unroll
-      for (int r = 0; r < R; ++r) tb[sw<LINES>(base + r * NS, line)] = v[b][r];
+      for (int r = 0; r < R; ++r) tb[sw<T, LINES>(base + r * NS, line)] = v[b][r];
     }
   }
   __syncthreads();
@@ -232,18 +243,18 @@ __device__ __forceinline__ void r2c_post(c2<T>* buf, const c2<T>* twN, int tid) 
     const int k = rest % (H / 2 + 1);
     c2<T>* tb = buf + (rest / (H / 2 + 1)) * TILE_ELEMS;
     if (k == 0) {
-      c2<T> y = tb[sw<LINES>(0, line)];
-      tb[sw<LINES>(0, line)] = mk<T>(y.x + y.y, y.x - y.y);
+      c2<T> y = tb[sw<T, LINES>(0, line)];
+      tb[sw<T, LINES>(0, line)] = mk<T>(y.x + y.y, y.x - y.y);
     } else {
-      const c2<T> yk = tb[sw<LINES>(k, line)];
-      const c2<T> yc = cconj<T>(tb[sw<LINES>(H - k, line)]);
+      const c2<T> yk = tb[sw<T, LINES>(k, line)];
+      const c2<T> yc = cconj<T>(tb[sw<T, LINES>(H - k, line)]);
       const c2<T> e = cscale<T>(cadd<T>(yk, yc), T(0.5));
       // O = (yk - yc) / (2i) = -i/2 (yk - yc)
       const c2<T> d = csub<T>(yk, yc);
       const c2<T> o = mk<T>(T(0.5) * d.y, T(-0.5) * d.x);
       const c2<T> wo = cmul<T>(o, twN[k]);
-      tb[sw<LINES>(k, line)] = cadd<T>(e, wo);
-      if (k != H - k) tb[sw<LINES>(H - k, line)] = cconj<T>(csub<T>(e, wo));
+      tb[sw<T, LINES>(k, line)] = cadd<T>(e, wo);
+      if (k != H - k) tb[sw<T, LINES>(H - k, line)] = cconj<T>(csub<T>(e, wo));
     }
   }
   __syncthreads();
@@ -262,16 +273,16 @@ __device__ __forceinline__ void c2r_pre(c2<T>* buf, const c2<T>* twN, int tid) {
     const int k = rest % (H / 2 + 1);
     c2<T>* tb = buf + (rest / (H / 2 + 1)) * TILE_ELEMS;
     if (k == 0) {
-      c2<T> x = tb[sw<LINES>(0, line)];  // (X0, XH)
-      tb[sw<LINES>(0, line)] = mk<T>(x.x + x.y, x.x - x.y);
+      c2<T> x = tb[sw<T, LINES>(0, line)];  // (X0, XH)
+      tb[sw<T, LINES>(0, line)] = mk<T>(x.x + x.y, x.x - x.y);
     } else {
-      const c2<T> a = tb[sw<LINES>(k, line)];
-      const c2<T> bc = cconj<T>(tb[sw<LINES>(H - k, line)]);
+      const c2<T> a = tb[sw<T, LINES>(k, line)];
+      const c2<T> bc = cconj<T>(tb[sw<T, LINES>(H - k, line)]);
       const c2<T> p = cadd<T>(a, bc);
       // q = i * W^{-k} (a - bc), W^{-k} = conj(twN[k])
       const c2<T> q = cmul_i<T>(cmulc<T>(csub<T>(a, bc), twN[k]));
-      tb[sw<LINES>(k, line)] = cadd<T>(p, q);
-      if (k != H - k) tb[sw<LINES>(H - k, line)] = cconj<T>(csub<T>(p, q));
+      tb[sw<T, LINES>(k, line)] = cadd<T>(p, q);
+      if (k != H - k) tb[sw<T, LINES>(H - k, line)] = cconj<T>(csub<T>(p, q));
     }
   }
   __syncthreads();
@@ -282,22 +293,46 @@ __device__ __forceinline__ void c2r_pre(c2<T>* buf, const c2<T>* twN, int tid) {
 // elements [0, E) of each row.  Row-major thread mapping: coalesced.
 template <typename T, typename G, int E, int LINES, int NT>
 __device__ __forceinline__ void load_rows(c2<T>* tile, const G* __restrict__ g, long ld, int tid) {
-  for (int idx = tid; idx < E * LINES; idx += NT) {
-    const int row = idx / E, m = idx % E;
-    const G v = g[row * ld + m];
-    tile[sw<LINES>(m, row)] = mk<T>(T(v.x), T(v.y));
+  if constexpr (std::is_same<T, float>::value && std::is_same<G, float2>::value && E % 2 == 0) {
+    // 16-byte loads of two consecutive elements (ld even, rows 16-byte aligned)
+    constexpr int E2 = E / 2;
+#pragma unroll 4
+    for (int idx = tid; idx < E2 * LINES; idx += NT) {
+      const int row = idx / E2, m2 = idx % E2;
+      const float4 v = reinterpret_cast<const float4*>(g + row * ld)[m2];
+      tile[sw<T, LINES>(2 * m2, row)] = make_float2(v.x, v.y);
+      tile[sw<T, LINES>(2 * m2 + 1, row)] = make_float2(v.z, v.w);
+    }
+  } else {
+#pragma unroll 4
+    for (int idx = tid; idx < E * LINES; idx += NT) {
+      const int row = idx / E, m = idx % E;
+      const G v = g[row * ld + m];
+      tile[sw<T, LINES>(m, row)] = mk<T>(T(v.x), T(v.y));
+    }
   }
 }
 
 template <typename T, typename G, int E, int LINES, int NT>
 __device__ __forceinline__ void store_rows(G* __restrict__ g, long ld, const c2<T>* tile, int tid) {
-  for (int idx = tid; idx < E * LINES; idx += NT) {
-    const int row = idx / E, m = idx % E;
-    const c2<T> v = tile[sw<LINES>(m, row)];
-    G o;
-    o.x = v.x;
-    o.y = v.y;
-    g[row * ld + m] = o;
+  if constexpr (std::is_same<T, float>::value && std::is_same<G, float2>::value && E % 2 == 0) {
+    constexpr int E2 = E / 2;
+#pragma unroll 4
+    for (int idx = tid; idx < E2 * LINES; idx += NT) {
+      const int row = idx / E2, m2 = idx % E2;
+      const float2 a0 = tile[sw<T, LINES>(2 * m2, row)], a1 = tile[sw<T, LINES>(2 * m2 + 1, row)];
+      reinterpret_cast<float4*>(g + row * ld)[m2] = make_float4(a0.x, a0.y, a1.x, a1.y);
+    }
+  } else {
+#pragma unroll 4
+    for (int idx = tid; idx < E * LINES; idx += NT) {
+      const int row = idx / E, m = idx % E;
+      const c2<T> v = tile[sw<T, LINES>(m, row)];
+      G o;
+      o.x = v.x;
+      o.y = v.y;
+      g[row * ld + m] = o;
+    }
   }
 }
 
@@ -306,20 +341,46 @@ __device__ __forceinline__ void store_rows(G* __restrict__ g, long ld, const c2<
 template <typename T, int L, int LINES, int NT>
 __device__ __forceinline__ void load_cols(c2<T>* tile, const c2<T>* __restrict__ g, long ld, int c0, int ncols,
                                           int tid) {
+  if constexpr (std::is_same<T, float>::value) {
+    if ((ld & 1) == 0 && (c0 & 1) == 0 && c0 + LINES <= ncols) {
+      // full tile of an even-width array: 16-byte loads of two adjacent lines
+#pragma unroll 4
+      for (int idx = tid; idx < L * (LINES / 2); idx += NT) {
+        const int m = idx / (LINES / 2), lp = idx % (LINES / 2);
+        const float4 v = *reinterpret_cast<const float4*>(g + m * ld + c0 + 2 * lp);
+        tile[sw<T, LINES>(m, 2 * lp)] = make_float2(v.x, v.y);
+        tile[sw<T, LINES>(m, 2 * lp + 1)] = make_float2(v.z, v.w);
+      }
+      return;
+    }
+  }
+#pragma unroll 4
   for (int idx = tid; idx < L * LINES; idx += NT) {
     const int m = idx / LINES, line = idx % LINES;
     const int c = c0 + line;
-    tile[sw<LINES>(m, line)] = (c < ncols) ? g[m * ld + c] : mk<T>(T(0), T(0));
+    tile[sw<T, LINES>(m, line)] = (c < ncols) ? g[m * ld + c] : mk<T>(T(0), T(0));
   }
 }
 
 template <typename T, int L, int LINES, int NT>
 __device__ __forceinline__ void store_cols(c2<T>* __restrict__ g, long ld, int c0, int ncols, const c2<T>* tile,
                                            int tid) {
+  if constexpr (std::is_same<T, float>::value) {
+    if ((ld & 1) == 0 && (c0 & 1) == 0 && c0 + LINES <= ncols) {
+#pragma unroll 4
+      for (int idx = tid; idx < L * (LINES / 2); idx += NT) {
+        const int m = idx / (LINES / 2), lp = idx % (LINES / 2);
+        const float2 a0 = tile[sw<T, LINES>(m, 2 * lp)], a1 = tile[sw<T, LINES>(m, 2 * lp + 1)];
+        *reinterpret_cast<float4*>(g + m * ld + c0 + 2 * lp) = make_float4(a0.x, a0.y, a1.x, a1.y);
+      }
+      return;
+    }
+  }
+#pragma unroll 4
   for (int idx = tid; idx < L * LINES; idx += NT) {
     const int m = idx / LINES, line = idx % LINES;
     const int c = c0 + line;
-    if (c < ncols) g[m * ld + c] = tile[sw<LINES>(m, line)];
+    if (c < ncols) g[m * ld + c] = tile[sw<T, LINES>(m, line)];
   }
 }
 

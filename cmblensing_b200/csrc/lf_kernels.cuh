@@ -79,6 +79,29 @@ __device__ __forceinline__ void store_io(void* p, int f64, long i, c2<T> v) {
   }
 }
 
+// Two consecutive packed elements: one 16-byte access for float32.
+template <typename T>
+__device__ __forceinline__ void ld2(const c2<T>* p, c2<T>* v) {
+  if constexpr (sizeof(c2<T>) == 8) {
+    const float4 w = *reinterpret_cast<const float4*>(p);
+    v[0] = mk<T>(T(w.x), T(w.y));
+    v[1] = mk<T>(T(w.z), T(w.w));
+  } else {
+    v[0] = p[0];
+    v[1] = p[1];
+  }
+}
+
+template <typename T>
+__device__ __forceinline__ void st2(c2<T>* p, const c2<T>* v) {
+  if constexpr (sizeof(c2<T>) == 8) {
+    *reinterpret_cast<float4*>(p) = make_float4(float(v[0].x), float(v[0].y), float(v[1].x), float(v[1].y));
+  } else {
+    p[0] = v[0];
+    p[1] = v[1];
+  }
+}
+
 template <typename T, int N, int NT>
 __device__ __forceinline__ void load_twiddles(c2<T>* tw, const void* g, int tid) {
   const c2<T>* src = reinterpret_cast<const c2<T>*>(g);
@@ -88,8 +111,8 @@ __device__ __forceinline__ void load_twiddles(c2<T>* tw, const void* g, int tid)
 // ======================================================== column pass
 // Gx = IFFT_col( (i KX / N^2) * FFT_col(S) ) on tiles of LINES columns.
 // grid: x = column tile (N/2/LINES), y = plane.
-template <typename T, int N, int LINES, int NT>
-__global__ void __launch_bounds__(NT) k_col(StageArgs a) {
+template <typename T, int N, int LINES, int NT, int MINB = 1>
+__global__ void __launch_bounds__(NT, MINB) k_col(StageArgs a) {
   constexpr int H = N / 2;
   extern __shared__ __align__(16) unsigned char smem_raw[];
   c2<T>* tw = reinterpret_cast<c2<T>*>(smem_raw);
@@ -109,8 +132,8 @@ __global__ void __launch_bounds__(NT) k_col(StageArgs a) {
     const int kx = (m < N / 2) ? m : m - N;
     T f = scale * T(kx);
     if (c0 + line == 0 && m == N / 2) f = T(0);  // packed DC/Nyquist line
-    const c2<T> v = buf[sw<LINES>(m, line)];
-    buf[sw<LINES>(m, line)] = mk<T>(-f * v.y, f * v.x);
+    const c2<T> v = buf[sw<T, LINES>(m, line)];
+    buf[sw<T, LINES>(m, line)] = mk<T>(-f * v.y, f * v.x);
   }
   __syncthreads();
   fft_tiles<T, N, LINES, 1, NT, true, N>(buf, tw, tid);
@@ -118,23 +141,27 @@ __global__ void __launch_bounds__(NT) k_col(StageArgs a) {
 }
 
 // ========================================================= row pass
-// One tile = LINES consecutive rows of one map; all C components.
+// One tile = LINES consecutive rows of one map, all C components at once, so
+// each phi pixel is read once per stage and applied to every component.
+// Shared memory holds 2C tiles: the "primary" tiles 0..C-1 and the
+// "secondary" tiles C..2C-1.
 // Standard RHS (lense_flow.py:365-370):  k = p_x d_x y + p_y d_y y
-// Adjoint RHS  (lense_flow.py:355-362):  k = d_x(p_x y) + d_y(p_y y)
-// RK4 (util.py:184-199): stage 1..3 accumulate k1 + 2 k2 + 2 k3 and form
-// the next stage input; stage 4 forms y0 + h/6 (acc + k4).
-// STAGE0 = true: initialisation (copy the input field, transform the first
-// stage input), no rate evaluation.
-// SAVE (reverse mode): the standard pass also stores d_x y_s and d_y y_s;
-// the adjoint pass stores its next stage input (the init pass its input).
-template <typename T, int N, int C, bool ADJ, bool STAGE0, int LINES, int NT, bool SAVE = false>
-__global__ void __launch_bounds__(NT) k_row(StageArgs a) {
+//   primary = Gx (column pass of S) -> d_x y;  secondary = S -> i KY S -> d_y y
+// Adjoint RHS (lense_flow.py:355-362):   k = d_x(p_x y) + d_y(p_y y)
+//   primary = Gx + i KY V (one inverse transform);  secondary = V
+// RK4 (util.py:184-199): stages 1..3 accumulate k1 + 2 k2 + 2 k3 and form the
+// next stage input; stage 4 forms y0 + h/6 (acc + k4).
+// STAGE0: initialisation (copy the input field, transform the first stage
+// input), no rate.  SAVE (reverse mode): the standard pass also stores
+// d_x y_s and d_y y_s; the adjoint pass stores its next stage input.
+template <typename T, int N, int C, bool ADJ, bool STAGE0, int LINES, int NT, bool SAVE = false, int MINB = 1>
+__global__ void __launch_bounds__(NT, MINB) k_row(StageArgs a) {
   constexpr int H = N / 2;
   constexpr long P = (long)N * N;
+  constexpr int TILE = LINES * H;
   extern __shared__ __align__(16) unsigned char smem_raw[];
   c2<T>* tw = reinterpret_cast<c2<T>*>(smem_raw);
-  c2<T>* buf0 = tw + N;
-  c2<T>* buf1 = buf0 + LINES * H;
+  c2<T>* buf = tw + N;  // tile t at buf + t * TILE
   const int tid = threadIdx.x;
   const int r0 = blockIdx.x * LINES;
   const long map = blockIdx.y;
@@ -144,134 +171,163 @@ __global__ void __launch_bounds__(NT) k_row(StageArgs a) {
   const T tcur = T(a.t_cur);
   const T hh = T(a.h);
   const T ky_scale = T(a.kbase / double(N));
+  const long half_plane = N * (long)H;  // complex elements per row-spectral plane
+  auto spec = [&](void* base, int c) {
+    return reinterpret_cast<c2<T>*>(base) + (map * C + c) * half_plane + (long)r0 * H;
+  };
+  auto real_rows = [&](void* base, int c) {
+    return reinterpret_cast<c2<T>*>(reinterpret_cast<T*>(base) + (map * C + c) * P + (long)r0 * N);
+  };
 
-#pragma unroll 1
-  for (int c = 0; c < C; ++c) {
-    const long plane = map * C + c;
-    const long prow = plane * P + (long)r0 * N;  // first pixel of the tile
-    c2<T>* sg = reinterpret_cast<c2<T>*>(a.s) + plane * (N * (long)H) + (long)r0 * H;
-    c2<T>* vg = reinterpret_cast<c2<T>*>(a.v) + plane * (N * (long)H) + (long)r0 * H;
-    const c2<T>* gg = reinterpret_cast<const c2<T>*>(a.gx) + plane * (N * (long)H) + (long)r0 * H;
-    c2<T>* y0g = reinterpret_cast<c2<T>*>(reinterpret_cast<T*>(a.y0) + prow);
-    c2<T>* accg = reinterpret_cast<c2<T>*>(reinterpret_cast<T*>(a.acc) + prow);
-
-    if constexpr (!STAGE0) {
-      // ------------------------------------------ rate from the spectra
-      load_rows<T, c2<T>, H, LINES, NT>(buf0, gg, H, tid);
-      load_rows<T, c2<T>, H, LINES, NT>(buf1, ADJ ? vg : sg, H, tid);
-      __syncthreads();
-      // d_y in the row spectrum: multiply by i KY / N (KY's DC and Nyquist
-      // bins contribute nothing after the inverse real transform).
-      for (int idx = tid; idx < H * LINES; idx += NT) {
-        const int row = idx / H, k = idx % H;
-        const c2<T> w = buf1[sw<LINES>(k, row)];
-        const T f = ky_scale * T(k);
-        const c2<T> dy = (k == 0) ? mk<T>(T(0), T(0)) : mk<T>(-f * w.y, f * w.x);
-        if constexpr (ADJ) {
-          // rate spectrum = Gx + i KY V / N  (one inverse transform)
-          const c2<T> g = buf0[sw<LINES>(k, row)];
-          buf0[sw<LINES>(k, row)] = (k == 0) ? g : cadd<T>(g, dy);
-        } else {
-          buf1[sw<LINES>(k, row)] = dy;
-        }
-      }
-      __syncthreads();
-      constexpr int NTI = ADJ ? 1 : 2;
-      c2r_pre<T, H, LINES, NTI, NT>(buf0, tw, tid);
-      fft_tiles<T, H, LINES, NTI, NT, true, N>(buf0, tw, tid);
-    } else {
-      // --------------------------------------------- initial input
-      const long fo = (map * C + c) * (P / 2) + (long)r0 * H;
-      for (int idx = tid; idx < H * LINES; idx += NT) {
-        const int row = idx / H, m = idx % H;
-        buf0[sw<LINES>(m, row)] = load_io<T>(a.f_in, a.in_f64, fo + (long)row * H + m);
-      }
-      __syncthreads();
+  // --------------------------------------------------------------- inputs
+  if constexpr (!STAGE0) {
+#pragma unroll
+    for (int c = 0; c < C; ++c) {
+      load_rows<T, c2<T>, H, LINES, NT>(buf + c * TILE, spec(a.gx, c), H, tid);
+      load_rows<T, c2<T>, H, LINES, NT>(buf + (C + c) * TILE, spec(ADJ ? a.v : a.s, c), H, tid);
     }
-
-    // ---------------------------------------------- pointwise epilogue
-    for (int idx = tid; idx < H * LINES; idx += NT) {
-      const int row = idx / H, m = idx % H;
-      const long e = (long)row * H + m;  // float2-element index within the tile
-      c2<T> ynext;
-      if constexpr (STAGE0) {
-        ynext = buf0[sw<LINES>(m, row)];
-        y0g[e] = ynext;
+    __syncthreads();
+    // d_y in the row spectrum: i KY / N (KY's DC and Nyquist bins contribute
+    // nothing after the inverse real transform)
+    for (int idx = tid; idx < H * LINES * C; idx += NT) {
+      const int c = idx / (H * LINES), rem = idx % (H * LINES);
+      const int row = rem / H, kk = rem % H;
+      c2<T>* sec = buf + (C + c) * TILE;
+      const c2<T> w = sec[sw<T, LINES>(kk, row)];
+      const T f = ky_scale * T(kk);
+      const c2<T> dy = (kk == 0) ? mk<T>(T(0), T(0)) : mk<T>(-f * w.y, f * w.x);
+      if constexpr (ADJ) {
+        c2<T>* pri = buf + c * TILE;
+        if (kk != 0) pri[sw<T, LINES>(kk, row)] = cadd<T>(pri[sw<T, LINES>(kk, row)], dy);
       } else {
-        const c2<T> g0 = buf0[sw<LINES>(m, row)];
-        c2<T> k;
-        if constexpr (ADJ) {
-          k = g0;
-        } else {
-          const c2<T> g1 = buf1[sw<LINES>(m, row)];
-          const c2<T> fx = reinterpret_cast<const c2<T>*>(phi)[e];
-          const c2<T> fy = reinterpret_cast<const c2<T>*>(phi + P)[e];
-          const c2<T> fxx = reinterpret_cast<const c2<T>*>(phi + 2 * P)[e];
-          const c2<T> fxy = reinterpret_cast<const c2<T>*>(phi + 3 * P)[e];
-          const c2<T> fyy = reinterpret_cast<const c2<T>*>(phi + 4 * P)[e];
-          T px, py;
-          p_vector<T>(fx.x, fy.x, fxx.x, fxy.x, fyy.x, tcur, px, py);
-          k.x = px * g0.x + py * g1.x;
-          p_vector<T>(fx.y, fy.y, fxx.y, fxy.y, fyy.y, tcur, px, py);
-          k.y = px * g0.y + py * g1.y;
-          if constexpr (SAVE) {
-            c2<T>* gs = reinterpret_cast<c2<T>*>(reinterpret_cast<T*>(a.grad) + plane * 2 * P + (long)r0 * N);
-            gs[e] = g0;
-            gs[P / 2 + e] = g1;
+        sec[sw<T, LINES>(kk, row)] = dy;
+      }
+    }
+    __syncthreads();
+    constexpr int NTI = ADJ ? C : 2 * C;
+    c2r_pre<T, H, LINES, NTI, NT>(buf, tw, tid);
+    fft_tiles<T, H, LINES, NTI, NT, true, N>(buf, tw, tid);
+  } else {
+    for (int idx = tid; idx < H * LINES * C; idx += NT) {
+      const int c = idx / (H * LINES), rem = idx % (H * LINES);
+      const int row = rem / H, m = rem % H;
+      const long fo = (map * C + c) * (P / 2) + (long)r0 * H + (long)row * H + m;
+      buf[c * TILE + sw<T, LINES>(m, row)] = load_io<T>(a.f_in, a.in_f64, fo);
+    }
+    __syncthreads();
+  }
+
+  // ---------------------------------------------------- pointwise epilogue
+  // Two packed elements (four pixels) per iteration; phi once for all C.
+  constexpr int E2 = H / 2;
+  const bool live = STAGE0 || !a.last;  // a next stage input is formed
+#pragma unroll 1
+  for (int idx = tid; idx < E2 * LINES; idx += NT) {
+    const int row = idx / E2, m0 = 2 * (idx % E2);
+    const long e0 = (long)row * H + m0;  // packed-element index within the tile
+    c2<T> fx[2], fy[2], fxx[2], fxy[2], fyy[2];
+    const bool need_phi = STAGE0 ? ADJ : (!ADJ || live);
+    if (need_phi) {
+      ld2<T>(reinterpret_cast<const c2<T>*>(phi) + e0, fx);
+      ld2<T>(reinterpret_cast<const c2<T>*>(phi + P) + e0, fy);
+      ld2<T>(reinterpret_cast<const c2<T>*>(phi + 2 * P) + e0, fxx);
+      ld2<T>(reinterpret_cast<const c2<T>*>(phi + 3 * P) + e0, fxy);
+      ld2<T>(reinterpret_cast<const c2<T>*>(phi + 4 * P) + e0, fyy);
+    }
+    // p at the rate time (standard) and at the next stage time (adjoint)
+    T prx[2][2], pry[2][2];
+    if (need_phi) {
+      const T tp = ADJ ? tnext : tcur;
+#pragma unroll
+      for (int q = 0; q < 2; ++q) {
+        p_vector<T>(fx[q].x, fy[q].x, fxx[q].x, fxy[q].x, fyy[q].x, tp, prx[q][0], pry[q][0]);
+        p_vector<T>(fx[q].y, fy[q].y, fxx[q].y, fxy[q].y, fyy[q].y, tp, prx[q][1], pry[q][1]);
+      }
+    }
+#pragma unroll
+    for (int c = 0; c < C; ++c) {
+      c2<T>* pri = buf + c * TILE;
+      c2<T>* sec = buf + (C + c) * TILE;
+      c2<T>* y0g = real_rows(a.y0, c);
+      c2<T>* accg = real_rows(a.acc, c);
+      c2<T> ynext[2];
+      if constexpr (STAGE0) {
+        ynext[0] = pri[sw<T, LINES>(m0, row)];
+        ynext[1] = pri[sw<T, LINES>(m0 + 1, row)];
+        st2<T>(y0g + e0, ynext);
+      } else {
+        c2<T> k[2], g0[2], g1[2];
+#pragma unroll
+        for (int q = 0; q < 2; ++q) {
+          g0[q] = pri[sw<T, LINES>(m0 + q, row)];
+          if constexpr (ADJ) {
+            k[q] = g0[q];
+          } else {
+            g1[q] = sec[sw<T, LINES>(m0 + q, row)];
+            k[q] = mk<T>(prx[q][0] * g0[q].x + pry[q][0] * g1[q].x, prx[q][1] * g0[q].y + pry[q][1] * g1[q].y);
           }
         }
-        const c2<T> y0 = y0g[e];
+        if constexpr (SAVE && !ADJ) {
+          c2<T>* gs = reinterpret_cast<c2<T>*>(reinterpret_cast<T*>(a.grad) + (map * C + c) * 2 * P + (long)r0 * N);
+          st2<T>(gs + e0, g0);
+          st2<T>(gs + P / 2 + e0, g1);
+        }
+        c2<T> y0[2], ac[2];
+        ld2<T>(y0g + e0, y0);
+        if (a.stage > 1) ld2<T>(accg + e0, ac);
         if (a.stage == 1) {
-          accg[e] = k;
-          ynext = mk<T>(y0.x + T(0.5) * hh * k.x, y0.y + T(0.5) * hh * k.y);
-        } else if (a.stage == 2) {
-          const c2<T> ac = accg[e];
-          accg[e] = mk<T>(ac.x + T(2) * k.x, ac.y + T(2) * k.y);
-          ynext = mk<T>(y0.x + T(0.5) * hh * k.x, y0.y + T(0.5) * hh * k.y);
-        } else if (a.stage == 3) {
-          const c2<T> ac = accg[e];
-          accg[e] = mk<T>(ac.x + T(2) * k.x, ac.y + T(2) * k.y);
-          ynext = mk<T>(y0.x + hh * k.x, y0.y + hh * k.y);
+#pragma unroll
+          for (int q = 0; q < 2; ++q)
+            ynext[q] = mk<T>(y0[q].x + T(0.5) * hh * k[q].x, y0[q].y + T(0.5) * hh * k[q].y);
+          st2<T>(accg + e0, k);
+        } else if (a.stage < 4) {
+          const T cc = a.stage == 2 ? T(0.5) * hh : hh;
+#pragma unroll
+          for (int q = 0; q < 2; ++q) {
+            ynext[q] = mk<T>(y0[q].x + cc * k[q].x, y0[q].y + cc * k[q].y);
+            ac[q] = mk<T>(ac[q].x + T(2) * k[q].x, ac[q].y + T(2) * k[q].y);
+          }
+          st2<T>(accg + e0, ac);
         } else {
-          const c2<T> ac = accg[e];
           const T h6 = hh / T(6);
-          ynext = mk<T>(y0.x + h6 * (ac.x + k.x), y0.y + h6 * (ac.y + k.y));
+#pragma unroll
+          for (int q = 0; q < 2; ++q)
+            ynext[q] = mk<T>(y0[q].x + h6 * (ac[q].x + k[q].x), y0[q].y + h6 * (ac[q].y + k[q].y));
           if (a.last) {
-            const long fo = (map * C + c) * (P / 2) + (long)r0 * H;
-            store_io<T>(a.f_out, a.out_f64, fo + e, ynext);
+            const long fo = (map * C + c) * (P / 2) + (long)r0 * H + e0;
+            store_io<T>(a.f_out, a.out_f64, fo, ynext[0]);
+            store_io<T>(a.f_out, a.out_f64, fo + 1, ynext[1]);
           } else {
-            y0g[e] = ynext;
+            st2<T>(y0g + e0, ynext);
           }
         }
       }
       if constexpr (SAVE && ADJ) {
-        if (STAGE0 || !a.last) reinterpret_cast<c2<T>*>(reinterpret_cast<T*>(a.dsave) + prow)[e] = ynext;
+        if (live) st2<T>(real_rows(a.dsave, c) + e0, ynext);
       }
-      if (STAGE0 || !a.last) {
-        if constexpr (ADJ) {
-          const c2<T> fx = reinterpret_cast<const c2<T>*>(phi)[e];
-          const c2<T> fy = reinterpret_cast<const c2<T>*>(phi + P)[e];
-          const c2<T> fxx = reinterpret_cast<const c2<T>*>(phi + 2 * P)[e];
-          const c2<T> fxy = reinterpret_cast<const c2<T>*>(phi + 3 * P)[e];
-          const c2<T> fyy = reinterpret_cast<const c2<T>*>(phi + 4 * P)[e];
-          T px0, py0, px1, py1;
-          p_vector<T>(fx.x, fy.x, fxx.x, fxy.x, fyy.x, tnext, px0, py0);
-          p_vector<T>(fx.y, fy.y, fxx.y, fxy.y, fyy.y, tnext, px1, py1);
-          buf0[sw<LINES>(m, row)] = mk<T>(px0 * ynext.x, px1 * ynext.y);
-          buf1[sw<LINES>(m, row)] = mk<T>(py0 * ynext.x, py1 * ynext.y);
-        } else {
-          buf0[sw<LINES>(m, row)] = ynext;
+      if (live) {
+#pragma unroll
+        for (int q = 0; q < 2; ++q) {
+          if constexpr (ADJ) {
+            pri[sw<T, LINES>(m0 + q, row)] = mk<T>(prx[q][0] * ynext[q].x, prx[q][1] * ynext[q].y);
+            sec[sw<T, LINES>(m0 + q, row)] = mk<T>(pry[q][0] * ynext[q].x, pry[q][1] * ynext[q].y);
+          } else {
+            pri[sw<T, LINES>(m0 + q, row)] = ynext[q];
+          }
         }
       }
     }
-    __syncthreads();
-    if (!STAGE0 && a.last) continue;  // uniform across the block
-    constexpr int NTO = ADJ ? 2 : 1;
-    fft_tiles<T, H, LINES, NTO, NT, false, N>(buf0, tw, tid);
-    r2c_post<T, H, LINES, NTO, NT>(buf0, tw, tid);
-    store_rows<T, c2<T>, H, LINES, NT>(sg, H, buf0, tid);
-    if constexpr (ADJ) store_rows<T, c2<T>, H, LINES, NT>(vg, H, buf1, tid);
-    __syncthreads();
+  }
+  if (!STAGE0 && a.last) return;  // uniform across the block
+  __syncthreads();
+  // ------------------------------------------------ next stage's spectra
+  constexpr int NTO = ADJ ? 2 * C : C;
+  fft_tiles<T, H, LINES, NTO, NT, false, N>(buf, tw, tid);
+  r2c_post<T, H, LINES, NTO, NT>(buf, tw, tid);
+#pragma unroll
+  for (int c = 0; c < C; ++c) {
+    store_rows<T, c2<T>, H, LINES, NT>(spec(a.s, c), H, buf + c * TILE, tid);
+    if constexpr (ADJ) store_rows<T, c2<T>, H, LINES, NT>(spec(a.v, c), H, buf + (C + c) * TILE, tid);
   }
 }
 
@@ -299,11 +355,11 @@ __global__ void __launch_bounds__(NT) k_phi_rows_r2c(const TI* __restrict__ phi,
     const int row = idx / (H + 1), k = idx % (H + 1);
     double2 v;
     if (k == 0) {
-      v = make_double2(buf[sw<LINES>(0, row)].x, 0.0);
+      v = make_double2(buf[sw<double, LINES>(0, row)].x, 0.0);
     } else if (k == H) {
-      v = make_double2(buf[sw<LINES>(0, row)].y, 0.0);
+      v = make_double2(buf[sw<double, LINES>(0, row)].y, 0.0);
     } else {
-      v = buf[sw<LINES>(k, row)];
+      v = buf[sw<double, LINES>(k, row)];
     }
     dst[(long)row * (H + 1) + k] = v;
   }
@@ -352,7 +408,7 @@ __global__ void __launch_bounds__(NT) k_phi_cols_deriv(const double2* __restrict
       const int col = c0 + line;
       const double kx = kbase * double(m < N / 2 ? m : m - N);
       const double ky = (col == H) ? -kbase * double(H) : kbase * double(col);
-      const double2 v = buf[sw<LINES>(m, line)];
+      const double2 v = buf[sw<double, LINES>(m, line)];
       double2 r;
       if (j == 0) r = make_double2(-kx * v.y * scale, kx * v.x * scale);
       else if (j == 1) r = make_double2(-ky * v.y * scale, ky * v.x * scale);
@@ -360,7 +416,7 @@ __global__ void __launch_bounds__(NT) k_phi_cols_deriv(const double2* __restrict
         const double f = (j == 2 ? -kx * kx : (j == 3 ? -kx * ky : -ky * ky)) * scale;
         r = make_double2(f * v.x, f * v.y);
       }
-      buf[sw<LINES>(m, line)] = r;
+      buf[sw<double, LINES>(m, line)] = r;
     }
     __syncthreads();
     fft_tiles<double, N, LINES, 1, NT, true, N>(buf, tw, tid);
@@ -368,7 +424,7 @@ __global__ void __launch_bounds__(NT) k_phi_cols_deriv(const double2* __restrict
     for (int idx = tid; idx < N * LINES; idx += NT) {
       const int m = idx / LINES, line = idx % LINES;
       const int col = c0 + line;
-      const double2 v = buf[sw<LINES>(m, line)];
+      const double2 v = buf[sw<double, LINES>(m, line)];
       if (col == 0) reinterpret_cast<double*>(out + (long)m * H)[0] = v.x;
       else if (col == H) reinterpret_cast<double*>(out + (long)m * H)[1] = v.x;
       else if (col < H) out[(long)m * H + col] = v;
@@ -506,8 +562,8 @@ __global__ void __launch_bounds__(NT) k_spec_cols_inv(const double2* __restrict_
   const double scale = 1.0 / (double(N) * double(N));
   for (int idx = tid; idx < N * LINES; idx += NT) {
     const int m = idx / LINES, line = idx % LINES;
-    const double2 v = buf[sw<LINES>(m, line)];
-    buf[sw<LINES>(m, line)] = make_double2(v.x * scale, v.y * scale);
+    const double2 v = buf[sw<double, LINES>(m, line)];
+    buf[sw<double, LINES>(m, line)] = make_double2(v.x * scale, v.y * scale);
   }
   __syncthreads();
   fft_tiles<double, N, LINES, 1, NT, true, N>(buf, tw, tid);
@@ -515,7 +571,7 @@ __global__ void __launch_bounds__(NT) k_spec_cols_inv(const double2* __restrict_
   for (int idx = tid; idx < N * LINES; idx += NT) {
     const int m = idx / LINES, line = idx % LINES;
     const int col = c0 + line;
-    const double2 v = buf[sw<LINES>(m, line)];
+    const double2 v = buf[sw<double, LINES>(m, line)];
     if (col == 0) reinterpret_cast<double*>(out + (long)m * H)[0] = v.x;
     else if (col == H) reinterpret_cast<double*>(out + (long)m * H)[1] = v.x;
     else if (col < H) out[(long)m * H + col] = v;
