@@ -123,13 +123,30 @@ class FlatS02(Field):
 
 
 # ------------------------------------------------------------- conversions
+def _fft_plan(m):
+    from . import engine
+    return engine.get_plan(m.shape[-2], 1, 1.0, "f64", device=m.device)
+
+
 def _rfft2(m):
-    return torch.fft.rfft2(m) if _is_torch(m) else np.fft.rfft2(m)
+    """rfft2; CUDA tensors go through the engine's float64 FFT kernels (lf_rfft2)."""
+    if _is_torch(m):
+        if m.is_cuda:
+            x = m if m.dtype in (torch.float32, torch.float64) else m.real
+            return _fft_plan(m).rfft2(x.reshape((-1,) + tuple(m.shape[-2:]))).reshape(
+                tuple(m.shape[:-1]) + (m.shape[-1] // 2 + 1,))
+        return torch.fft.rfft2(m)
+    return np.fft.rfft2(m)
 
 
 def _irfft2(m):
+    """irfft2; CUDA tensors go through the engine's float64 FFT kernels (lf_irfft2)."""
     n = m.shape[-2]
-    return torch.fft.irfft2(m, s=(n, n)) if _is_torch(m) else np.fft.irfft2(m, s=(n, n))
+    if _is_torch(m):
+        if m.is_cuda:
+            return _fft_plan(m).irfft2(m.reshape((-1,) + tuple(m.shape[-2:]))).reshape(tuple(m.shape[:-1]) + (n,))
+        return torch.fft.irfft2(m, s=(n, n))
+    return np.fft.irfft2(m, s=(n, n))
 
 
 def fourier(field):
@@ -142,16 +159,29 @@ def map(field):  # noqa: A001  (name kept from fields.py:168)
     return field.replace(basis=Basis.MAP, **{n: _irfft2(getattr(field, n)) for n in field._matrix_names()})
 
 
+_ANGLES = {}
+
+
 def _eb_angle(nside, theta_pix, like=None):
-    d = math.radians(theta_pix / ARCMIN_PER_DEGREE)
-    lx = 2 * np.pi * np.fft.rfftfreq(nside, d)
-    ly = 2 * np.pi * np.fft.fftfreq(nside, d)
-    lx, ly = np.meshgrid(lx, ly)
-    lx[: nside // 2 + 1, -1] *= -1  # util.py:143
-    a = np.arctan2(lx, ly)
+    """arctan2(lx, ly) on the rfft2 grid with the reference's Nyquist flip (util.py:140-149)."""
+    key = (int(nside), float(theta_pix))
+    a = _ANGLES.get(key)
+    if a is None:
+        d = math.radians(theta_pix / ARCMIN_PER_DEGREE)
+        lx = 2 * np.pi * np.fft.rfftfreq(nside, d)
+        ly = 2 * np.pi * np.fft.fftfreq(nside, d)
+        lx, ly = np.meshgrid(lx, ly)
+        lx[: nside // 2 + 1, -1] *= -1  # util.py:143
+        a = np.arctan2(lx, ly)
+        _ANGLES[key] = a
     if _is_torch(like):
-        return torch.as_tensor(a, device=like.device)
-    return a
+        dkey = key + (str(like.device),)
+        t = _ANGLES.get(dkey)
+        if t is None:
+            t = (torch.as_tensor(np.cos(2 * a), device=like.device), torch.as_tensor(np.sin(2 * a), device=like.device))
+            _ANGLES[dkey] = t
+        return t
+    return np.cos(2 * a), np.sin(2 * a)
 
 
 def eb2qu(field):
@@ -159,8 +189,7 @@ def eb2qu(field):
     if isinstance(field, FlatS0):
         return field
     e, b = field.polar_matrix_1, field.polar_matrix_2
-    a = _eb_angle(field.nside, field.theta_pix, e)
-    c2a, s2a = (torch.cos(2 * a), torch.sin(2 * a)) if _is_torch(a) else (np.cos(2 * a), np.sin(2 * a))
+    c2a, s2a = _eb_angle(field.nside, field.theta_pix, e)
     return field.replace(polar_matrix_1=-e * c2a + b * s2a, polar_matrix_2=-e * s2a - b * c2a,
                          parametrization=Parametrization.QU)
 
@@ -170,10 +199,22 @@ def qu2eb(field):
     if isinstance(field, FlatS0):
         return field
     q, u = field.polar_matrix_1, field.polar_matrix_2
-    a = _eb_angle(field.nside, field.theta_pix, q)
-    c2a, s2a = (torch.cos(2 * a), torch.sin(2 * a)) if _is_torch(a) else (np.cos(2 * a), np.sin(2 * a))
+    c2a, s2a = _eb_angle(field.nside, field.theta_pix, q)
     return field.replace(polar_matrix_1=-q * c2a - u * s2a, polar_matrix_2=q * s2a - u * c2a,
                          parametrization=Parametrization.EB)
+
+
+def undo_inner_product(field):
+    """fields.py:147-154: identity for Fourier-shaped matrices, else irfft2(conj(rfft2(m) / w) N^2)."""
+    def _undo(m):
+        if m.shape[-2] != m.shape[-1]:
+            return m
+        w = field.fourier_weights
+        if _is_torch(m):
+            w = torch.as_tensor(w, device=m.device)
+            return _irfft2(torch.conj(_rfft2(m) / w) * field.nside ** 2)
+        return _irfft2(np.conj(_rfft2(m) / w) * field.nside ** 2)
+    return field.replace(**{n: _undo(getattr(field, n)) for n in field._matrix_names()})
 
 
 def dot(field_1, field_2):

@@ -44,3 +44,42 @@ def lense_flow(field, phi, n=10, direction=1, adjoint=False, precision="f32"):
     else:
         upd = {nm: out[0, i] for i, nm in enumerate(names)}
     return field.replace(**upd)
+
+
+def _stack(field, dev):
+    mats = [torch.as_tensor(getattr(field, nm), device=dev) for nm in field._matrix_names()]
+    t = torch.stack(mats).unsqueeze(0)
+    return t if t.dtype in (torch.float32, torch.float64) else t.real.to(torch.float64)
+
+
+def lense_flow_backwards(transformed_field, phi, cotangent, n=10, direction=1, swap_qu=True, precision="f32"):
+    """The reference's custom-VJP backward pass (cmb_lensing/lense_flow.py:23-46).
+
+    Integrates (f, delta_f, delta_phi) from the lensed field in the opposite
+    time direction on the GPU (lf_lense_flow_vjp) and returns
+    ``(undo_inner_product(delta_field), undo_inner_product(delta_phi))``.
+    With ``swap_qu`` the Q/U matrices of delta_field are returned swapped, as
+    the reference's output_like_input writes them (lense_flow.py:143-144,
+    151-152); pass ``swap_qu=False`` for the mathematically ordered result.
+    """
+    from .fields import FlatS0, undo_inner_product
+    names = transformed_field._matrix_names()
+    m0 = getattr(transformed_field, names[0])
+    host = not isinstance(m0, torch.Tensor)
+    dev = m0.device if not host and m0.is_cuda else _device()
+    fl = _stack(transformed_field, dev).to(torch.float64)
+    ct = _stack(cotangent, dev).to(torch.float64)
+    pm = torch.as_tensor(phi.scalar_matrix, device=dev)
+    fourier_phi = pm.shape[-1] != pm.shape[-2]
+    pm = pm.to(torch.complex128) if fourier_phi else pm.to(torch.float64)
+    plan = engine.get_plan(fl.shape[-1], fl.shape[1], phi.pix_width, precision, device=dev)
+    planes = plan.phi_planes(pm.unsqueeze(0), check_det=False)
+    df, dphi = plan.lense_flow_vjp(fl, ct, planes, n=n, direction=direction,
+                                   phi_basis="fourier" if fourier_phi else "map")
+    comps = [df[0, i] for i in range(len(names))]
+    if swap_qu and not isinstance(transformed_field, FlatS0):
+        comps[-2], comps[-1] = comps[-1], comps[-2]
+    conv = (lambda t: t.cpu().numpy()) if host else (lambda t: t)
+    dfield = transformed_field.replace(**{nm: conv(c) for nm, c in zip(names, comps)})
+    dphi_field = phi.replace(scalar_matrix=conv(dphi[0]))
+    return undo_inner_product(dfield), undo_inner_product(dphi_field)

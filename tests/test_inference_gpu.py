@@ -1,0 +1,95 @@
+"""GPU parity of logpdf, gradf_logpdf, grad_phi_logpdf and the Wiener filter against the oracle.
+
+Inputs are the reference's golden fixtures (256^2, 2.5', T and QU sets) with
+DC/Nyquist Fourier weight 1; n = 7.  Tolerances: FP32 lensing gives ~1e-7
+relative error in the lensed field, so logpdf agrees to 1e-9 relative,
+gradf and grad_phi to 2e-5 relative L2.
+"""
+import numpy as np
+import pytest
+
+from conftest import load_golden, rel_l2
+from oracle import lenseflow_ref as R
+
+pytestmark = pytest.mark.gpu
+N = 256
+
+
+@pytest.fixture(scope="module")
+def torch_cuda():
+    import torch
+    if not torch.cuda.is_available():
+        pytest.skip("no CUDA device")
+    return torch
+
+
+def _sets(which, mod):
+    """(golden, kwargs) for module ``mod`` (the oracle or cmblensing_b200)."""
+    gl = load_golden("lens_I.npz" if which == "I" else "lens_P.npz")
+    g = load_golden("infer_I.npz" if which == "I" else "infer_P.npz")
+    w = R.get_fourier_weights((N, N))
+    kw = dict(fourier_weights=w)
+    if which == "I":
+        D = lambda m: mod.DiagonalScalar(scalar_matrix=m, **kw)
+        S = dict(field=mod.FlatS0(scalar_matrix=gl["t"], **kw), phi=mod.FlatS0(scalar_matrix=gl["phi"], **kw),
+                 data=mod.FlatS0(scalar_matrix=g["data_t"], **kw), Cn=D(g["cn"]), Cphi=D(g["cphi"]), Cf=D(g["cf"]),
+                 M=D(g["m"]), B=D(g["b"]))
+    else:
+        D = lambda p: mod.DiagonalEB(matrix_EE=g[p + "_ee"], matrix_BB=g[p + "_bb"], **kw)
+        S = dict(field=mod.FlatS2(polar_matrix_1=gl["e"], polar_matrix_2=gl["b"], **kw),
+                 phi=mod.FlatS0(scalar_matrix=gl["phi"], **kw),
+                 data=mod.FlatS2(polar_matrix_1=g["data_e"], polar_matrix_2=g["data_b"], **kw),
+                 Cn=D("cn"), Cphi=mod.DiagonalScalar(scalar_matrix=g["cphi"], **kw), Cf=D("cf"), M=D("m"), B=D("b"))
+    return g, S
+
+
+class _Mod:
+    """cmblensing_b200's containers under the oracle's names."""
+    def __init__(self):
+        import cmblensing_b200 as cl
+        from cmblensing_b200 import matrix_operators as mo
+        self.FlatS0, self.FlatS2, self.FlatS02 = cl.FlatS0, cl.FlatS2, cl.FlatS02
+        self.DiagonalScalar, self.DiagonalEB, self.BlockTEB = mo.DiagonalScalar, mo.DiagonalEB, mo.BlockTEB
+
+
+@pytest.mark.parametrize("which", ["I", "P"])
+def test_logpdf(torch_cuda, which):
+    from cmblensing_b200.statistics import logpdf
+    g, S = _sets(which, _Mod())
+    v = logpdf(S["field"], S["phi"], S["data"], S["Cn"], S["Cphi"], S["Cf"], S["M"], S["B"], n=7)
+    _, So = _sets(which, R)
+    ref = R.logpdf(So["field"], So["phi"], So["data"], So["Cn"], So["Cphi"], So["Cf"], So["M"], So["B"], n=7)
+    assert abs(v - ref) / abs(ref) < 1e-9
+    assert abs(v - float(g["logpdf"])) / abs(float(g["logpdf"])) < 1e-9  # the Julia golden
+
+
+@pytest.mark.parametrize("which", ["I", "P"])
+def test_gradf_logpdf(torch_cuda, which):
+    from cmblensing_b200.gradients import gradf_logpdf
+    _, S = _sets(which, _Mod())
+    out = gradf_logpdf(S["field"], S["phi"], S["data"], S["Cf"], S["Cn"], S["M"], S["B"], n=7)
+    _, So = _sets(which, R)
+    ref = R.gradf_logpdf(So["field"], So["phi"], So["data"], So["Cf"], So["Cn"], So["M"], So["B"], n=7)
+    for nm in ref._matrix_names():
+        assert rel_l2(getattr(out, nm), getattr(ref, nm)) < 2e-5
+
+
+@pytest.mark.parametrize("which", ["I", "P"])
+def test_grad_phi_logpdf(torch_cuda, which):
+    from cmblensing_b200.gradients import grad_phi_logpdf
+    _, S = _sets(which, _Mod())
+    out = grad_phi_logpdf(S["field"], S["phi"], S["data"], S["Cn"], S["Cphi"], S["Cf"], S["M"], S["B"], n=7)
+    _, So = _sets(which, R)
+    ref = R.grad_phi_logpdf(So["field"], So["phi"], So["data"], So["Cn"], So["Cphi"], So["Cf"], So["M"], So["B"], n=7)
+    assert rel_l2(out.scalar_matrix, ref) < 2e-5
+
+
+def test_wiener_filter_reference_rule(torch_cuda):
+    """The reference's stopping rule (r.z < 0.1, 500 iterations), T set, n = 7: same iterate as the oracle PCG."""
+    from cmblensing_b200.wiener_filter import wiener_filter
+    _, S = _sets("I", _Mod())
+    out = wiener_filter(S["data"] * 0, S["phi"], S["data"], S["Cf"], S["Cn"], S["M"], S["B"], n=7, maxiter=8)
+    _, So = _sets("I", R)
+    ref, _ = R.wiener_filter(So["data"] * 0, So["phi"], So["data"], So["Cf"], So["Cn"], So["M"], So["B"], n=7,
+                             maxiter=8)
+    assert rel_l2(out.scalar_matrix, ref.scalar_matrix) < 1e-4
