@@ -49,7 +49,7 @@ def on_device(fn):
         dev = None
         conv = []
         for a in args:
-            if hasattr(a, "_matrix_names"):
+            if hasattr(a, "_matrix_names") and not isinstance(getattr(a, a._matrix_names()[0]), (int, float)):
                 m = getattr(a, a._matrix_names()[0])
                 if not (isinstance(m, torch.Tensor) and m.is_cuda):
                     host = True

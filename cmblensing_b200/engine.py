@@ -217,39 +217,98 @@ class Plan:
 
 
 class HostPipeline:
-    """The reference-facing call with host buffers, for a fixed batch.
+    """The reference-facing call with host buffers, for a fixed batch, pipelined.
 
-    Each call copies f [B,C,N,N] and phi [B,N,N] (float64, pinned host) to the
+    Each call copies f [B,C,N,N] and phi [B,N,N] (pinned host memory) to the
     device, computes the phi derivative planes (with the magnification check),
-    lenses, and copies the result back into a pinned host buffer.  Device
-    buffers are allocated once.
+    lenses, and copies the result back into a pinned host buffer.  The batch
+    is split into ``chunks``: the host-to-device copy of chunk i+1, the compute
+    of chunk i and the device-to-host copy of chunk i-1 run on three streams
+    at once, with double-buffered device slots.  The magnification minima are
+    read back once per call, after the last chunk; a call whose phi is
+    singular raises SingularMagnificationError (its outputs are then
+    meaningless).  Device buffers are allocated once.
     """
 
-    def __init__(self, plan, batch, io_dtype=torch.float64):
+    def __init__(self, plan, batch, io_dtype=torch.float64, chunks=4):
         self.plan = plan
         N, C = plan.nside, plan.ncomp
         dev = plan.device
         self.batch = batch
-        self.d_f = torch.empty((batch, C, N, N), dtype=io_dtype, device=dev)
-        self.d_out = torch.empty_like(self.d_f)
-        self.d_phi = torch.empty((batch, N, N), dtype=torch.float64, device=dev)
-        self.planes = torch.empty((batch, 5, N, N), dtype=plan.dtype, device=dev)
-        self.ws = torch.empty(max(plan.workspace_bytes(batch, True), 16), dtype=torch.uint8, device=dev)
-        self.phi_ws = torch.empty(max(plan.phi_workspace_bytes(batch), 16), dtype=torch.uint8, device=dev)
+        self.chunks = max(1, min(int(chunks), batch))
+        self.cb = -(-batch // self.chunks)  # maps per chunk (last may be shorter)
+        cb = self.cb
+        self.io_dtype = io_dtype
+        self.d_f = [torch.empty((cb, C, N, N), dtype=io_dtype, device=dev) for _ in range(2)]
+        self.d_out = [torch.empty((cb, C, N, N), dtype=io_dtype, device=dev) for _ in range(2)]
+        self.d_phi = [torch.empty((cb, N, N), dtype=torch.float64, device=dev) for _ in range(2)]
+        self.planes = torch.empty((cb, 5, N, N), dtype=plan.dtype, device=dev)
+        self.ws = torch.empty(max(plan.workspace_bytes(cb, True), 16), dtype=torch.uint8, device=dev)
+        self.phi_ws = torch.empty(max(plan.phi_workspace_bytes(cb), 16), dtype=torch.uint8, device=dev)
+        self.min_det = torch.empty(max(self.chunks * cb, 1), dtype=torch.int32, device=dev)
+        self.s_in = torch.cuda.Stream(dev)
+        self.s_cmp = torch.cuda.Stream(dev)
+        self.s_out = torch.cuda.Stream(dev)
 
     def h2d_bytes(self):
-        return self.d_f.numel() * self.d_f.element_size() + self.d_phi.numel() * 8
+        N, C = self.plan.nside, self.plan.ncomp
+        return self.batch * (C * N * N * torch.tensor([], dtype=self.io_dtype).element_size() + N * N * 8)
 
     def d2h_bytes(self):
-        return self.d_out.numel() * self.d_out.element_size()
+        N, C = self.plan.nside, self.plan.ncomp
+        return self.batch * C * N * N * torch.tensor([], dtype=self.io_dtype).element_size()
 
     def __call__(self, f_host, phi_host, out_host, n=10, direction=FORWARD_LENSE, adjoint=False, check_det=True):
-        self.d_f.copy_(f_host, non_blocking=True)
-        self.d_phi.copy_(phi_host, non_blocking=True)
-        self.plan.phi_planes(self.d_phi, check_det=check_det, out=self.planes, workspace=self.phi_ws)
-        self.plan.lense_flow(self.d_f, self.planes, n=n, direction=direction, adjoint=adjoint, out=self.d_out,
-                             workspace=self.ws)
-        out_host.copy_(self.d_out, non_blocking=True)
+        plan, lib = self.plan, self.plan._lib
+        cur = torch.cuda.current_stream(plan.device)
+        for st in (self.s_in, self.s_cmp, self.s_out):
+            st.wait_stream(cur)
+        if check_det:
+            with torch.cuda.stream(self.s_cmp):
+                nat.check(lib.lf_min_det_init(_ptr(self.min_det), self.min_det.numel(), _stream_ptr(plan.device)),
+                          "lf_min_det_init")
+        ev_in = [torch.cuda.Event() for _ in range(self.chunks)]
+        ev_cmp = [torch.cuda.Event() for _ in range(self.chunks)]
+        ev_out = [torch.cuda.Event() for _ in range(self.chunks)]
+        N, C = plan.nside, plan.ncomp
+        for i in range(self.chunks):
+            lo, hi = i * self.cb, min((i + 1) * self.cb, self.batch)
+            m = hi - lo
+            if m <= 0:
+                break
+            slot = i % 2
+            with torch.cuda.stream(self.s_in):
+                if i >= 2:
+                    self.s_in.wait_event(ev_cmp[i - 2])  # the slot's previous chunk has been consumed
+                self.d_f[slot][:m].copy_(f_host[lo:hi], non_blocking=True)
+                self.d_phi[slot][:m].copy_(phi_host[lo:hi], non_blocking=True)
+                ev_in[i].record(self.s_in)
+            with torch.cuda.stream(self.s_cmp):
+                self.s_cmp.wait_event(ev_in[i])
+                if i >= 2:
+                    self.s_cmp.wait_event(ev_out[i - 2])  # the slot's previous output has been copied out
+                st = _stream_ptr(plan.device)
+                md = _ptr(self.min_det[lo:]) if check_det else None
+                nat.check(lib.lf_phi_precompute(plan.handle, _ptr(self.d_phi[slot]), nat.LF_PHI_MAP, m,
+                                                _ptr(self.planes), md, _ptr(self.phi_ws), self.phi_ws.numel(), st),
+                          "lf_phi_precompute")
+                code = nat.LF_F64 if self.io_dtype == torch.float64 else nat.LF_F32
+                nat.check(lib.lf_lense_flow(plan.handle, _ptr(self.d_f[slot]), code, _ptr(self.d_out[slot]), code,
+                                            _ptr(self.planes), m, int(n), int(direction), int(bool(adjoint)),
+                                            _ptr(self.ws), self.ws.numel(), st), "lf_lense_flow")
+                ev_cmp[i].record(self.s_cmp)
+            with torch.cuda.stream(self.s_out):
+                self.s_out.wait_event(ev_cmp[i])
+                out_host[lo:hi].copy_(self.d_out[slot][:m], non_blocking=True)
+                ev_out[i].record(self.s_out)
+        for st in (self.s_in, self.s_cmp, self.s_out):
+            cur.wait_stream(st)
+        if check_det:
+            vals = [lib.lf_decode_min_det(int(v)) for v in self.min_det[:self.batch].cpu().tolist()]
+            plan.last_min_det = vals
+            if not all(v > 0.0 for v in vals):
+                raise nat.SingularMagnificationError(nat.LF_ERR_SINGULAR_MAGNIFICATION,
+                                                     f"min det(I + t grad grad phi) = {min(vals):.3g}")
         return out_host
 
 

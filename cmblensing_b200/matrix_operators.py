@@ -86,6 +86,8 @@ class DiagonalScalar(FieldOperator):
         return ["scalar_matrix"]
 
     def __mul__(self, other):
+        if isinstance(other, (PixelMask, ComposedOperator)):
+            return ComposedOperator([self]) * other
         if isinstance(other, DiagonalScalar):
             return self.replace(scalar_matrix=self.scalar_matrix * other.scalar_matrix)
         if isinstance(other, FlatS0):
@@ -105,6 +107,8 @@ class DiagonalEB(FieldOperator):
         return ["matrix_EE", "matrix_BB"]
 
     def __mul__(self, other):
+        if isinstance(other, (PixelMask, ComposedOperator)):
+            return ComposedOperator([self]) * other
         if isinstance(other, DiagonalEB):
             return self.replace(matrix_EE=self.matrix_EE * other.matrix_EE, matrix_BB=self.matrix_BB * other.matrix_BB)
         if isinstance(other, FlatS2):
@@ -129,6 +133,8 @@ class BlockTEB(FieldOperator):
 
     def __mul__(self, other):
         s = self
+        if isinstance(other, (PixelMask, ComposedOperator)):
+            return ComposedOperator([self]) * other
         if isinstance(other, BlockTEB):
             o = other
             return s.replace(matrix_TT=s.matrix_TT * o.matrix_TT + s.matrix_TE * o.matrix_ET,
@@ -146,6 +152,62 @@ class BlockTEB(FieldOperator):
         if isinstance(other, BlockTEB):
             return other.__mul__(self)
         return self.replace(**{n: getattr(self, n) * other for n in self._matrix_names()})
+
+
+# ------------------------------------------------- map-space masks (extension)
+@dataclasses.dataclass
+class PixelMask(FieldOperator):
+    """Multiplication by a real (N, N) map in pixel space, acting on Fourier fields.
+
+    Not in the reference, whose masks are Fourier-diagonal (``DiagonalEB``);
+    used for masks with holes.  On an EB (or T) Fourier field it applies
+    qu2eb(fourier(m * map(eb2qu(f)))), so it slots into the reference's
+    formulas (gradients.py:17-25) unchanged.  Products with diagonal operators
+    become ``ComposedOperator``s applied right to left.
+    """
+    mask_map: object = None
+
+    def _matrix_names(self):
+        return ["mask_map"]
+
+    def apply(self, field):
+        from .fields import eb2qu, fourier, map, qu2eb
+        mp = map(eb2qu(field))
+        mp = mp.replace(**{n: getattr(mp, n) * self.mask_map for n in mp._matrix_names()})
+        return qu2eb(fourier(mp))
+
+    def __mul__(self, other):
+        if isinstance(other, (FlatS0, FlatS2, FlatS02)):
+            return self.apply(other)
+        if isinstance(other, FieldOperator) or isinstance(other, ComposedOperator):
+            return ComposedOperator([self]) * other
+        return self.replace(mask_map=self.mask_map * other)
+
+    def diagonal_like(self, op):
+        """A Fourier-diagonal stand-in of the same kind as ``op`` with value sqrt(mean(m^2)) (for preconditioners)."""
+        m = self.mask_map
+        v = float((m * m).mean()) ** 0.5
+        ones = lambda a: (a * 0 + 1) * v
+        return op.replace(**{n: ones(getattr(op, n)) for n in op._matrix_names()})
+
+
+class ComposedOperator:
+    """A product of operators, applied right to left to a field."""
+
+    def __init__(self, ops):
+        self.ops = list(ops)
+
+    def __mul__(self, other):
+        if isinstance(other, (FlatS0, FlatS2, FlatS02)):
+            out = other
+            for op in reversed(self.ops):
+                out = op * out
+            return out
+        if isinstance(other, ComposedOperator):
+            return ComposedOperator(self.ops + other.ops)
+        if isinstance(other, (FieldOperator, PixelMask)):
+            return ComposedOperator(self.ops + [other])
+        return ComposedOperator(self.ops[:-1] + [self.ops[-1] * other])
 
 
 def pinv(op):

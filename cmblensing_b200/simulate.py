@@ -130,3 +130,75 @@ def lens_batch(nside, theta_pix, batch, ncomp, seed0=0):
             f[i, ncomp - 2] = q
             f[i, ncomp - 1] = u
     return f, phis
+
+
+# ------------------------------------------------- inference problems
+def _cl_grid(cl, nside, theta_pix):
+    ell, d = ell_grid(nside, theta_pix)
+    with np.errstate(divide="ignore", invalid="ignore"):
+        return np.where(ell > 0, cl(np.where(ell > 0, ell, 1.0)), 0.0) / d ** 2
+
+
+def beam_grid(nside, theta_pix, fwhm_arcmin):
+    """B(l) = exp(-l^2 sigma^2 / 2), sigma = FWHM / sqrt(8 ln 2), zero at l = 0 (simulate.py:133-138)."""
+    ell, _ = ell_grid(nside, theta_pix)
+    sig = fwhm_arcmin * ARCMIN / math.sqrt(8 * math.log(2))
+    b = np.exp(-(ell ** 2) * sig ** 2 / 2)
+    b[0, 0] = 0.0
+    return b
+
+
+def hole_mask(nside, theta_pix, nholes=30, rmin=5.0, rmax=20.0, apod=10.0, seed=5000):
+    """Pixel mask with ``nholes`` circular holes (radius rmin..rmax arcmin) and a cosine taper of ``apod`` arcmin."""
+    rng = np.random.default_rng(seed)
+    size = nside * theta_pix
+    y, x = np.meshgrid(np.arange(nside) * theta_pix, np.arange(nside) * theta_pix, indexing="ij")
+    m = np.ones((nside, nside))
+    for _ in range(nholes):
+        cy, cx = rng.uniform(0, size, 2)
+        r = rng.uniform(rmin, rmax)
+        dy = np.minimum(np.abs(y - cy), size - np.abs(y - cy))  # periodic flat sky
+        dx = np.minimum(np.abs(x - cx), size - np.abs(x - cx))
+        d = np.sqrt(dx ** 2 + dy ** 2)
+        w = np.where(d <= r, 0.0, np.where(d >= r + apod, 1.0, 0.5 * (1 - np.cos(np.pi * (d - r) / apod))))
+        m *= w
+    return m
+
+
+def inference_problem(nside, theta_pix, beam_fwhm=3.0, noise_t=10.0, noise_p=14.0, seed=0, bb_fraction=0.0):
+    """Host arrays of a lensed-CMB inference problem in the reference's units and layouts.
+
+    Returns a dict with the unlensed fields ``t, e, b`` and the potential
+    ``phi`` as unnormalised rfft2 arrays, noise realisations ``n_t, n_e, n_b``
+    (white, ``noise_*`` uK-arcmin), and the Fourier-diagonal ``cf_tt, cf_ee,
+    cf_bb, cn_t, cn_p, cphi, beam``.  Covariances are C_l / d^2
+    (simulate.py:71-97) scaled by the factors the fields were rescaled by.
+    The caller forms the data d = B L(phi) f + n with the lensing operator.
+    The simulated B is zero; ``bb_fraction`` sets the prior C_BB to that
+    fraction of C_EE (with C_BB = 0 the reference's pinv leaves B modes with
+    no prior, and a masked Wiener filter is then nearly singular).
+    """
+    rng_seed = seed
+    f_t = gaussian_field(nside, theta_pix, "TT", seed=2000 + rng_seed)
+    f_e = gaussian_field(nside, theta_pix, "EE", seed=2500 + rng_seed)
+    phi = gaussian_phi(nside, theta_pix, seed=1000 + rng_seed)
+    # covariances with the normalisations the fields were rescaled by
+    def scaled_cov(kind, fmap, seedv):
+        raw = _grf(SPECTRA[kind], nside, theta_pix, np.random.default_rng(seedv))
+        s = (RMS_UK[kind] / np.sqrt(np.mean(raw ** 2))) ** 2
+        return _cl_grid(SPECTRA[kind], nside, theta_pix) * s
+    cf_tt = scaled_cov("TT", f_t, 2000 + rng_seed)
+    cf_ee = scaled_cov("EE", f_e, 2500 + rng_seed)
+    raw_phi = _grf(phi_spectrum(), nside, theta_pix, np.random.default_rng(1000 + rng_seed))
+    sphi = (2.5 * ARCMIN / deflection_rms(raw_phi, theta_pix)) ** 2
+    cphi = _cl_grid(phi_spectrum(), nside, theta_pix) * sphi
+    shape = cf_tt.shape
+    out = dict(t=np.fft.rfft2(f_t), e=np.fft.rfft2(f_e), b=np.zeros(shape, complex), phi=np.fft.rfft2(phi),
+               cf_tt=cf_tt, cf_ee=cf_ee, cf_bb=bb_fraction * cf_ee, cphi=cphi,
+               cn_t=np.full(shape, (noise_t / theta_pix) ** 2), cn_p=np.full(shape, (noise_p / theta_pix) ** 2),
+               beam=beam_grid(nside, theta_pix, beam_fwhm), nside=nside, theta_pix=theta_pix)
+    rng = np.random.default_rng(3000 + rng_seed)
+    out["n_t"] = np.fft.rfft2(rng.standard_normal((nside, nside)) * noise_t / theta_pix)
+    out["n_e"] = np.fft.rfft2(rng.standard_normal((nside, nside)) * noise_p / theta_pix)
+    out["n_b"] = np.fft.rfft2(rng.standard_normal((nside, nside)) * noise_p / theta_pix)
+    return out

@@ -20,7 +20,7 @@ import math
 from ._device import on_device
 from .fields import dot
 from .gradients import gradf_logpdf
-from .matrix_operators import pinv
+from .matrix_operators import PixelMask, pinv
 
 
 def get_b_vector(phi, data, field_covariance, noise_covariance, mask, beam, n=10, precision="f32"):
@@ -30,7 +30,13 @@ def get_b_vector(phi, data, field_covariance, noise_covariance, mask, beam, n=10
 
 
 def hessian_logpdf_preconditioner(field_covariance, beam, mask, noise_covariance):
-    """wiener_filter.py:36-43: Cf^-1 + B M Cn^-1 M B (Fourier-diagonal)."""
+    """wiener_filter.py:36-43: Cf^-1 + B M Cn^-1 M B (Fourier-diagonal).
+
+    A map-space ``PixelMask`` enters through its Fourier-diagonal stand-in
+    sqrt(mean(m^2)) (the preconditioner must stay diagonal).
+    """
+    if isinstance(mask, PixelMask):
+        mask = mask.diagonal_like(beam)
     return pinv(field_covariance) + beam * mask * pinv(noise_covariance) * mask * beam
 
 

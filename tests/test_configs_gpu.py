@@ -1,0 +1,199 @@
+"""The gradient and Wiener-filter workloads on the GPU.
+
+Gradient workload: 256^2 IQU, 3' pixels, d = B L(phi) f + n with a 3' FWHM
+beam and white noise of 10 / 14 uK-arcmin (T / QU), no mask, n = 7.  The
+FP32 gradients are checked against the float64 oracle's restatement of the
+reference (tolerance 2e-5) and against central finite differences of
+logpdf (eps = 1e-3 rms) along 16 seeded directions.  For f, logpdf is
+quadratic and the gradient uses the exact discrete adjoint: 1e-4.  For phi,
+the reference's continuous delta-phi adjoint differs from the exact
+derivative by the RK4 discretisation error: 5e-3.  Directions are seeded
+Gaussian random fields with the workload's spectra.
+
+Wiener-filter workload: 512^2 QU, 2' pixels, 1' beam, 2 uK-arcmin noise, a
+pixel mask with 30 apodised holes, B-mode prior at 1% of C_EE (the
+simulated B is zero); FP32 operator, float64 inner products, true-residual
+refinement every 10 iterations.  Stopped at ||r||/||b|| = 1e-8, the
+solution must agree with the FP64-engine solution (stopped at 1e-10) to
+1e-6.  The 64^2 case compares the GPU PCG with the oracle's float64 PCG.
+"""
+import numpy as np
+import pytest
+
+from conftest import rel_l2
+from oracle import lenseflow_ref as R
+
+pytestmark = pytest.mark.gpu
+
+
+@pytest.fixture(scope="module")
+def torch_cuda():
+    import torch
+    if not torch.cuda.is_available():
+        pytest.skip("no CUDA device")
+    return torch
+
+
+def _problem(mod, N, theta, pol, beam_fwhm, noise_t, noise_p, seed=0, nlens=7, mask=None, bb_fraction=0.0):
+    """Reference-shaped fields/operators for module ``mod`` (oracle R or cmblensing_b200), data lensed by the oracle."""
+    from cmblensing_b200.simulate import inference_problem
+    p = inference_problem(N, theta, beam_fwhm=beam_fwhm, noise_t=noise_t, noise_p=noise_p, seed=seed,
+                          bb_fraction=bb_fraction)
+    pw = R.pix_width_of(theta)
+    w = R.get_fourier_weights((N, N))
+    kw = dict(nside=N, theta_pix=theta, pix_width=pw, fourier_weights=w)
+    ones = np.ones_like(p["beam"])
+    if pol == "IP":
+        field = mod.FlatS02(scalar_matrix=p["t"], polar_matrix_1=p["e"], polar_matrix_2=p["b"], **kw)
+        Z = np.zeros_like(ones)
+        blk = lambda tt, ee, bb: mod.BlockTEB(matrix_TT=tt, matrix_TE=Z, matrix_ET=Z, matrix_EE=ee, matrix_BB=bb, **kw)
+        Cf = blk(p["cf_tt"], p["cf_ee"], p["cf_bb"])
+        Cn = blk(p["cn_t"], p["cn_p"], p["cn_p"])
+        B = blk(p["beam"], p["beam"], p["beam"])
+        M = blk(ones, ones, ones)
+        noise = mod.FlatS02(scalar_matrix=p["n_t"], polar_matrix_1=p["n_e"], polar_matrix_2=p["n_b"], **kw)
+    else:
+        field = mod.FlatS2(polar_matrix_1=p["e"], polar_matrix_2=p["b"], **kw)
+        eb = lambda ee, bb: mod.DiagonalEB(matrix_EE=ee, matrix_BB=bb, **kw)
+        Cf = eb(p["cf_ee"], p["cf_bb"])
+        Cn = eb(p["cn_p"], p["cn_p"])
+        B = eb(p["beam"], p["beam"])
+        M = eb(ones, ones)
+        noise = mod.FlatS2(polar_matrix_1=p["n_e"], polar_matrix_2=p["n_b"], **kw)
+    phi = mod.FlatS0(scalar_matrix=p["phi"], **kw)
+    Cphi = mod.DiagonalScalar(scalar_matrix=p["cphi"], **kw)
+    # data with the oracle: d = B L f + n (Fourier-diagonal M = 1 here)
+    fo = R.FlatS02 if pol == "IP" else R.FlatS2
+    f_or = fo(**{k: getattr(field, k) for k in field._matrix_names()}, nside=N, theta_pix=theta, pix_width=pw,
+              fourier_weights=w)
+    lensed = R.qu2eb(R.fourier(R.lense_flow(R.map_(R.eb2qu(f_or)), R.FlatS0(scalar_matrix=p["phi"], nside=N,
+                                                                               theta_pix=theta, pix_width=pw), n=nlens)))
+    dmat = {k: p["beam"] * getattr(lensed, k) + getattr(noise, k) for k in field._matrix_names()}
+    if mask is not None:  # pixel-space mask on the data
+        from cmblensing_b200 import matrix_operators as mo
+        M = mo.PixelMask(mask_map=mask, **kw)
+        mq = R.map_(R.eb2qu(fo(**dmat, nside=N, theta_pix=theta, pix_width=pw, fourier_weights=w)))
+        dm = R.qu2eb(R.fourier(mq.replace(**{k: getattr(mq, k) * mask for k in mq._matrix_names()})))
+        dmat = {k: getattr(dm, k) for k in field._matrix_names()}
+    data = field.replace(**dmat)
+    return dict(field=field, phi=phi, data=data, Cf=Cf, Cn=Cn, B=B, M=M, Cphi=Cphi)
+
+
+def _as_oracle(S):
+    """The same problem as oracle containers."""
+    conv = {}
+    for k, v in S.items():
+        cls = getattr(R, type(v).__name__)
+        conv[k] = cls(**{f: getattr(v, f) for f in v._matrix_names()}, nside=v.nside, theta_pix=v.theta_pix,
+                      pix_width=v.pix_width, fourier_weights=v.fourier_weights)
+    return conv
+
+
+def _direction(field, seed, kind):
+    """A seeded Gaussian-random-field direction with the workload's spectra, in the field's Fourier basis.
+
+    ``kind`` "f": TT for T and EE for E and B; "phi": the phi spectrum.  (Pixel-scale white-noise
+    directions in phi are where the reference's continuous delta-phi adjoint is least accurate.)
+    """
+    from cmblensing_b200.simulate import gaussian_field, gaussian_phi
+    N, th = field.nside, field.theta_pix
+    mats = {}
+    for i, k in enumerate(field._matrix_names()):
+        if kind == "phi":
+            m = gaussian_phi(N, th, seed=seed)
+        else:
+            m = gaussian_field(N, th, "TT" if k == "scalar_matrix" else "EE", seed=seed + 97 * i)
+        mats[k] = np.fft.rfft2(m / np.sqrt(np.mean(m ** 2)))
+    return field.replace(**mats)
+
+
+def test_gradients_256_IQU(torch_cuda):
+    import cmblensing_b200 as cl
+    from cmblensing_b200 import matrix_operators as mo
+    from cmblensing_b200.gradients import grad_phi_logpdf, gradf_logpdf
+    from cmblensing_b200.statistics import logpdf
+
+    class Mod:
+        FlatS0, FlatS2, FlatS02 = cl.FlatS0, cl.FlatS2, cl.FlatS02
+        DiagonalScalar, DiagonalEB, BlockTEB = mo.DiagonalScalar, mo.DiagonalEB, mo.BlockTEB
+
+    S = _problem(Mod, 256, 3.0, "IP", 3.0, 10.0, 14.0, seed=1)
+    So = _as_oracle(S)
+    f, phi, d = S["field"], S["phi"], S["data"]
+    gf = gradf_logpdf(f, phi, d, S["Cf"], S["Cn"], S["M"], S["B"], n=7)
+    gf_ref = R.gradf_logpdf(So["field"], So["phi"], So["data"], So["Cf"], So["Cn"], So["M"], So["B"], n=7)
+    for k in gf_ref._matrix_names():
+        assert rel_l2(getattr(gf, k), getattr(gf_ref, k)) < 2e-5
+    gp = grad_phi_logpdf(f, phi, d, S["Cn"], S["Cphi"], S["Cf"], S["M"], S["B"], n=7)
+    gp_ref = R.grad_phi_logpdf(So["field"], So["phi"], So["data"], So["Cn"], So["Cphi"], So["Cf"], So["M"], So["B"],
+                               n=7)
+    assert rel_l2(gp.scalar_matrix, gp_ref) < 2e-5
+
+    def lp(ff, pp):
+        # float64 engine for the finite differences themselves
+        from cmblensing_b200 import lense_flow as lfm
+        old = lfm.engine.lense_flow_batch
+        try:
+            lfm.engine.lense_flow_batch = lambda *a, **k: old(*a, **{**k, "precision": "f64"})
+            return logpdf(ff, pp, d, S["Cn"], S["Cphi"], S["Cf"], S["M"], S["B"], n=7)
+        finally:
+            lfm.engine.lense_flow_batch = old
+
+    rms_f = np.sqrt(np.mean(np.fft.irfft2(f.scalar_matrix, s=(256, 256)) ** 2))
+    rms_p = np.sqrt(np.mean(np.fft.irfft2(phi.scalar_matrix, s=(256, 256)) ** 2))
+    errs_f, errs_p = [], []
+    for k in range(16):
+        v = _direction(f, 4000 + k, "f")
+        eps = 1e-3 * rms_f
+        fd = (lp(f + v * eps, phi) - lp(f - v * eps, phi)) / (2 * eps)
+        errs_f.append((fd, R.dot(gf, v)))
+        u = _direction(phi, 4100 + k, "phi")
+        eps = 1e-3 * rms_p
+        fd = (lp(f, phi + u * eps) - lp(f, phi - u * eps)) / (2 * eps)
+        errs_p.append((fd, R.dot(gp, u)))
+    # errors relative to the typical directional derivative (a direction whose own derivative is
+    # small would otherwise dominate a per-direction ratio)
+    for pairs, tol in ((errs_f, 1e-4), (errs_p, 5e-3)):
+        scale = np.sqrt(np.mean([a * a for a, _ in pairs]))
+        worst = max(abs(a - b) for a, b in pairs) / scale
+        assert worst < tol, (worst, pairs)
+
+
+def test_wiener_filter_64_matches_oracle_pcg(torch_cuda):
+    """The GPU PCG (FP32 operator, float64 dots) against the oracle's float64 PCG, same stopping rule."""
+    import cmblensing_b200 as cl
+    from cmblensing_b200 import matrix_operators as mo
+    from cmblensing_b200.wiener_filter import wiener_filter
+
+    class Mod:
+        FlatS0, FlatS2, FlatS02 = cl.FlatS0, cl.FlatS2, cl.FlatS02
+        DiagonalScalar, DiagonalEB, BlockTEB = mo.DiagonalScalar, mo.DiagonalEB, mo.BlockTEB
+
+    S = _problem(Mod, 64, 2.0, "P", 1.0, 2.0, 2.0, seed=3, bb_fraction=0.01)
+    So = _as_oracle(S)
+    x = wiener_filter(S["data"] * 0, S["phi"], S["data"], S["Cf"], S["Cn"], S["M"], S["B"], n=7, rel_tol=1e-8,
+                      refine_every=10)
+    xo, _ = R.wiener_filter(So["data"] * 0, So["phi"], So["data"], So["Cf"], So["Cn"], So["M"], So["B"], n=7,
+                            rel_tol=1e-10)
+    for k in xo._matrix_names():
+        assert rel_l2(getattr(x, k), getattr(xo, k)) < 1e-6
+
+
+def test_wiener_filter_512_QU_masked(torch_cuda):
+    import cmblensing_b200 as cl
+    from cmblensing_b200 import matrix_operators as mo
+    from cmblensing_b200.simulate import hole_mask
+    from cmblensing_b200.wiener_filter import wiener_filter
+
+    class Mod:
+        FlatS0, FlatS2, FlatS02 = cl.FlatS0, cl.FlatS2, cl.FlatS02
+        DiagonalScalar, DiagonalEB, BlockTEB = mo.DiagonalScalar, mo.DiagonalEB, mo.BlockTEB
+
+    mask = hole_mask(512, 2.0)
+    S = _problem(Mod, 512, 2.0, "P", 1.0, 2.0, 2.0, seed=2, mask=mask, bb_fraction=0.01)
+    args = (S["data"] * 0, S["phi"], S["data"], S["Cf"], S["Cn"], S["M"], S["B"])
+    x32 = wiener_filter(*args, n=7, rel_tol=1e-8, refine_every=10, return_iterations=True, maxiter=1000)
+    it32 = wiener_filter.last_iterations
+    x64 = wiener_filter(*args, n=7, rel_tol=1e-10, precision="f64", maxiter=2000)
+    for k in x64._matrix_names():
+        assert rel_l2(getattr(x32, k), getattr(x64, k)) < 1e-6, (k, it32)

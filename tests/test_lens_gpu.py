@@ -246,3 +246,37 @@ def test_reference_shaped_api(torch_cuda):
     ref = _oracle(f[0], phis[0], pw, 7, -1, False)
     assert rel_l2(out.polar_matrix_1, ref[0]) < TOL32
     assert rel_l2(out.polar_matrix_2, ref[1]) < TOL32
+
+
+@pytest.mark.parametrize("B,chunks", [(5, 2), (8, 4)])
+def test_host_pipeline_matches_device_call(torch_cuda, B, chunks):
+    """The pipelined host-buffer path (three streams, double-buffered chunks) equals the device call per map."""
+    import torch
+    from cmblensing_b200 import engine
+    f, phis = _inputs(128, 3.0, 2, B=B)
+    pw = R.pix_width_of(3.0)
+    plan = engine.get_plan(128, 2, pw)
+    pipe = engine.HostPipeline(plan, B, chunks=chunks)
+    fh = torch.from_numpy(f).pin_memory()
+    ph = torch.from_numpy(phis).pin_memory()
+    oh = torch.empty_like(fh).pin_memory()
+    for _ in range(2):  # second call reuses every slot
+        pipe(fh, ph, oh, n=7)
+        torch.cuda.synchronize()
+    ref = plan.lense_flow(torch.as_tensor(f, device="cuda"), plan.phi_planes(torch.as_tensor(phis, device="cuda")),
+                          n=7)
+    assert torch.equal(oh, ref.cpu())
+
+
+def test_host_pipeline_reports_singular_phi(torch_cuda):
+    import torch
+    from cmblensing_b200 import _native as nat
+    from cmblensing_b200 import engine
+    from cmblensing_b200.simulate import gaussian_phi
+    f, phis = _inputs(128, 3.0, 1, B=3)
+    phis[1] = gaussian_phi(128, 3.0, seed=7, spectrum="literal")
+    plan = engine.get_plan(128, 1, R.pix_width_of(3.0))
+    pipe = engine.HostPipeline(plan, 3, chunks=3)
+    with pytest.raises(nat.SingularMagnificationError):
+        pipe(torch.from_numpy(f).pin_memory(), torch.from_numpy(phis).pin_memory(),
+             torch.empty(f.shape, dtype=torch.float64).pin_memory(), n=7)
