@@ -1,0 +1,326 @@
+"""Device-resident continuous-batching service for lens, delens and Wiener-filter requests.
+
+Requests of mixed grid sizes arrive as they like (``Server.submit``).  A
+scheduler thread admits them against an HBM budget, groups lens and delens
+requests by (N, components, direction) and launches each group as one
+batched engine call into a *slot*: static device buffers plus a CUDA graph
+of the phi-derivative precompute and the LenseFlow launch sequence,
+captured once per batch-size bucket and replayed afterwards.  Every slot has
+its own stream, so batches of different shapes run concurrently on the
+device; while they run, newly arrived requests queue for the next batch of
+their group.  A batch's completion event frees its slot and memory and
+completes its requests.  Wiener-filter solves (data-dependent CG iteration
+counts) run eagerly on worker threads, each with its own stream.
+
+Each lensed map is computed by exactly the kernels and tiles it would use
+alone, so a request's result is bit-identical whether it runs alone or in a
+mix (tested).
+"""
+from __future__ import annotations
+
+import collections
+import queue
+import threading
+import time
+
+import numpy as np
+import torch
+
+from . import _native as nat
+from . import engine
+from .simulate import ARCMIN
+
+_req_ids = iter(range(1 << 62))
+
+
+class Request:
+    """One unit of work.  ``kind`` is "lens", "delens" or "wf".
+
+    lens/delens: ``f`` [C, N, N] and ``phi`` [N, N] host float arrays.
+    wf: ``problem`` = dict(field, phi, data, Cf, Cn, M, B) of reference-shaped
+    containers (host arrays), solved with ``wf_kwargs``.
+    """
+
+    def __init__(self, kind, nside, ncomp, theta_pix, f=None, phi=None, problem=None, n=7, wf_kwargs=None):
+        self.id = next(_req_ids)
+        self.kind = kind
+        self.nside = int(nside)
+        self.ncomp = int(ncomp)
+        self.theta_pix = float(theta_pix)
+        self.f = f
+        self.phi = phi
+        self.problem = problem
+        self.n = n
+        self.wf_kwargs = wf_kwargs or {}
+        self.t_submit = None
+        self.t_done = None
+        self.result = None
+        self.error = None
+        self.done = threading.Event()
+
+    @property
+    def latency(self):
+        return None if self.t_done is None else self.t_done - self.t_submit
+
+    def footprint(self):
+        """Device bytes this request holds while in flight (inputs, outputs, planes, workspaces)."""
+        N, C = self.nside, self.ncomp
+        P = N * N
+        if self.kind == "wf":
+            return 64 * C * P + 120 * P  # fields, spectra and two lens workspaces in float64/float32
+        return 8 * C * P * 2 + 8 * P + 20 * P + 20 * C * P + 48 * P
+
+
+def _bucket(b):
+    s = 1
+    while s < b:
+        s *= 2
+    return s
+
+
+class _LensSlot:
+    """Static buffers, stream and captured graphs for batches of one (N, C, direction)."""
+
+    def __init__(self, dev, nside, ncomp, theta_pix, direction, cap, n, use_graphs):
+        self.dev = dev
+        self.nside, self.ncomp, self.direction, self.cap, self.n = nside, ncomp, direction, cap, n
+        self.plan = engine.get_plan(nside, ncomp, theta_pix * ARCMIN, "f32", device=dev)
+        N, C = nside, ncomp
+        self.h_f = torch.empty((cap, C, N, N), dtype=torch.float32).pin_memory()
+        self.h_phi = torch.empty((cap, N, N), dtype=torch.float64).pin_memory()
+        self.h_out = torch.empty((cap, C, N, N), dtype=torch.float32).pin_memory()
+        self.h_md = torch.empty(cap, dtype=torch.int32).pin_memory()
+        self.d_f = torch.empty((cap, C, N, N), dtype=torch.float32, device=dev)
+        self.d_phi = torch.empty((cap, N, N), dtype=torch.float64, device=dev)
+        self.d_out = torch.empty_like(self.d_f)
+        self.planes = torch.empty((cap, 5, N, N), dtype=torch.float32, device=dev)
+        self.ws = torch.empty(max(self.plan.workspace_bytes(cap, True), 16), dtype=torch.uint8, device=dev)
+        self.phi_ws = torch.empty(max(self.plan.phi_workspace_bytes(cap), 16), dtype=torch.uint8, device=dev)
+        self.md = torch.empty(cap, dtype=torch.int32, device=dev)
+        self.stream = torch.cuda.Stream(dev)
+        self.graphs = {}
+        self.use_graphs = use_graphs
+        self.busy = False
+        self.event = None
+        self.reqs = []
+
+    def _body(self, b):
+        p, lib = self.plan, self.plan._lib
+        st = engine._stream_ptr(self.dev)
+        nat.check(lib.lf_min_det_init(engine._ptr(self.md), b, st), "lf_min_det_init")
+        nat.check(lib.lf_phi_precompute(p.handle, engine._ptr(self.d_phi), nat.LF_PHI_MAP, b, engine._ptr(self.planes),
+                                        engine._ptr(self.md), engine._ptr(self.phi_ws), self.phi_ws.numel(), st),
+                  "lf_phi_precompute")
+        nat.check(lib.lf_lense_flow(p.handle, engine._ptr(self.d_f), nat.LF_F32, engine._ptr(self.d_out), nat.LF_F32,
+                                    engine._ptr(self.planes), b, self.n, self.direction, 0, engine._ptr(self.ws),
+                                    self.ws.numel(), st), "lf_lense_flow")
+
+    def launch(self, reqs):
+        """Copy inputs in, run (graph replay or eager) and copy outputs out, all on this slot's stream."""
+        b = len(reqs)
+        self.reqs = reqs
+        self.busy = True
+        for i, r in enumerate(reqs):
+            self.h_f[i].copy_(torch.from_numpy(np.asarray(r.f, dtype=np.float32)))
+            self.h_phi[i].copy_(torch.from_numpy(np.asarray(r.phi, dtype=np.float64)))
+        with torch.cuda.stream(self.stream):
+            self.d_f[:b].copy_(self.h_f[:b], non_blocking=True)
+            self.d_phi[:b].copy_(self.h_phi[:b], non_blocking=True)
+            bb = _bucket(b) if self.use_graphs else b
+            bb = min(bb, self.cap)
+            if self.use_graphs:
+                g = self.graphs.get(bb)
+                if g is None:
+                    self._body(bb)  # eager warm-up: kernel attributes are set outside the capture
+                    g = torch.cuda.CUDAGraph()
+                    # thread-local capture: Wiener-filter workers keep running on their own threads
+                    with torch.cuda.graph(g, stream=self.stream, capture_error_mode="thread_local"):
+                        self._body(bb)
+                    self.graphs[bb] = g
+                g.replay()
+            else:
+                self._body(b)
+            self.h_out[:b].copy_(self.d_out[:b], non_blocking=True)
+            self.h_md[:b].copy_(self.md[:b], non_blocking=True)
+            self.event = torch.cuda.Event()
+            self.event.record(self.stream)
+
+    def poll(self):
+        """Complete the batch's requests if its event has fired; return them."""
+        if not self.busy or not self.event.query():
+            return []
+        lib = self.plan._lib
+        now = time.perf_counter()
+        out = self.h_out[:len(self.reqs)].numpy().copy()
+        mds = self.h_md[:len(self.reqs)].tolist()
+        done = self.reqs
+        for i, r in enumerate(done):
+            md = lib.lf_decode_min_det(int(mds[i]))
+            if not md > 0.0:
+                r.error = nat.SingularMagnificationError(nat.LF_ERR_SINGULAR_MAGNIFICATION, f"min det {md:.3g}")
+            else:
+                r.result = out[i]
+            r.t_done = now
+            r.done.set()
+        self.busy = False
+        self.reqs = []
+        return done
+
+
+class Server:
+    """Continuous-batching scheduler over the LenseFlow engine on one GPU."""
+
+    def __init__(self, hbm_budget=32 << 30, max_batch=16, use_graphs=True, wf_workers=4, device=None):
+        self.dev = torch.device("cuda", torch.cuda.current_device() if device is None else torch.device(device).index)
+        self.budget = int(hbm_budget)
+        self.max_batch = int(max_batch)
+        self.use_graphs = use_graphs
+        self.inbox = queue.Queue()
+        self.pending = collections.defaultdict(collections.deque)  # group key -> requests
+        self.slots = {}  # group key -> list of _LensSlot
+        self.in_use = 0
+        self.wf_queue = queue.Queue()
+        self.completed = []
+        self._stop = threading.Event()
+        self._lock = threading.Lock()
+        self._thread = threading.Thread(target=self._loop, daemon=True)
+        self._wf_threads = [threading.Thread(target=self._wf_loop, daemon=True) for _ in range(wf_workers)]
+
+    # ------------------------------------------------------------ client
+    def start(self):
+        self._thread.start()
+        for t in self._wf_threads:
+            t.start()
+        return self
+
+    def submit(self, req):
+        req.t_submit = time.perf_counter()
+        self.inbox.put(req)
+        return req
+
+    def stop(self):
+        self._stop.set()
+        self._thread.join()
+        for _ in self._wf_threads:
+            self.wf_queue.put(None)
+        for t in self._wf_threads:
+            t.join()
+
+    # ---------------------------------------------------------- internal
+    def _release(self, nbytes):
+        with self._lock:
+            self.in_use -= nbytes
+
+    def _admit(self, nbytes):
+        with self._lock:
+            if self.in_use + nbytes > self.budget and self.in_use > 0:
+                return False
+            self.in_use += nbytes
+            return True
+
+    def _finish(self, reqs):
+        for r in reqs:
+            self._release(r.footprint())
+        self.completed.extend(reqs)
+
+    def _slot_for(self, key):
+        for s in self.slots.setdefault(key, []):
+            if not s.busy:
+                return s
+        if len(self.slots[key]) < 2:  # two slots per shape: one can fill while the other runs
+            N, C, th, direction = key
+            s = _LensSlot(self.dev, N, C, th, direction, self.max_batch, 7, self.use_graphs)
+            self.slots[key].append(s)
+            return s
+        return None
+
+    def _loop(self):
+        torch.cuda.set_device(self.dev)
+        waiting = collections.deque()  # admitted-later requests in arrival order
+        while not self._stop.is_set() or any(self.pending.values()) or any(
+                s.busy for ss in self.slots.values() for s in ss):
+            # 1. retire finished batches
+            for ss in self.slots.values():
+                for s in ss:
+                    self._finish(s.poll())
+            # 2. take arrivals
+            try:
+                while True:
+                    waiting.append(self.inbox.get_nowait())
+            except queue.Empty:
+                pass
+            # 3. admit by footprint, in arrival order
+            while waiting and self._admit(waiting[0].footprint()):
+                r = waiting.popleft()
+                if r.kind == "wf":
+                    self.wf_queue.put(r)
+                else:
+                    d = nat_direction(r.kind)
+                    self.pending[(r.nside, r.ncomp, r.theta_pix, d)].append(r)
+            # 4. launch every group that has work and a free slot
+            launched = False
+            for key, q in self.pending.items():
+                if not q:
+                    continue
+                s = self._slot_for(key)
+                if s is None:
+                    continue
+                batch = [q.popleft() for _ in range(min(len(q), self.max_batch))]
+                try:
+                    s.launch(batch)
+                except Exception as e:  # surface errors per request, keep serving
+                    for r in batch:
+                        r.error = e
+                        r.t_done = time.perf_counter()
+                        r.done.set()
+                    s.busy = False
+                    self._finish(batch)
+                launched = True
+            if not launched:
+                time.sleep(0.0002)
+
+    def _wf_loop(self):
+        from .wiener_filter import wiener_filter
+        torch.cuda.set_device(self.dev)
+        stream = torch.cuda.Stream(self.dev)
+        while True:
+            r = self.wf_queue.get()
+            if r is None:
+                return
+            try:
+                with torch.cuda.stream(stream):
+                    P = r.problem
+                    r.result = wiener_filter(P["data"] * 0, P["phi"], P["data"], P["Cf"], P["Cn"], P["M"], P["B"],
+                                             n=r.n, **r.wf_kwargs)
+                    torch.cuda.current_stream().synchronize()
+            except Exception as e:
+                r.error = e
+            r.t_done = time.perf_counter()
+            r.done.set()
+            self._finish([r])
+
+
+def nat_direction(kind):
+    return 1 if kind == "lens" else -1
+
+
+def run_alone(req):
+    """The same request executed by itself with plain engine calls (no batching, no graphs)."""
+    if req.kind == "wf":
+        from .wiener_filter import wiener_filter
+        P = req.problem
+        return wiener_filter(P["data"] * 0, P["phi"], P["data"], P["Cf"], P["Cn"], P["M"], P["B"], n=req.n,
+                             **req.wf_kwargs)
+    plan = engine.get_plan(req.nside, req.ncomp, req.theta_pix * ARCMIN, "f32")
+    f = torch.as_tensor(np.asarray(req.f, dtype=np.float32), device="cuda").unsqueeze(0)
+    phi = torch.as_tensor(np.asarray(req.phi, dtype=np.float64), device="cuda").unsqueeze(0)
+    planes = plan.phi_planes(phi, check_det=True)
+    return plan.lense_flow(f, planes, n=req.n, direction=nat_direction(req.kind))[0].cpu().numpy()
+
+
+def latency_summary(reqs):
+    lat = np.array([r.latency for r in reqs if r.latency is not None])
+    if lat.size == 0:
+        return {}
+    return {"p50_ms": float(np.percentile(lat, 50) * 1e3), "p99_ms": float(np.percentile(lat, 99) * 1e3),
+            "mean_ms": float(lat.mean() * 1e3), "n": int(lat.size)}
