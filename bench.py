@@ -49,6 +49,8 @@ def parse():
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-fp64", action="store_true")
     ap.add_argument("--no-e2e", action="store_true")
+    ap.add_argument("--serving-seconds", type=float, default=1.5)
+    ap.add_argument("--serving-rate", type=float, default=200.0)
     return ap.parse_args()
 
 
@@ -222,6 +224,112 @@ def survey_bytes_per_map(C, n, P):
     return (4 * n * (36 * C + 20) + 8 * C + 140) * P
 
 
+
+# ----------------------------------------------------------------- serving
+SERVE_SIZES = {128: 3.0, 256: 3.0, 512: 2.0, 1024: 2.0}
+
+
+def _wf_problem(N, C, theta, seed):
+    """A Wiener-filter request's problem: beam 1', noise 2 (QU) / 10 (T) uK', hole mask, data lensed by the engine."""
+    import numpy as np
+    import torch
+    import cmblensing_b200 as cl
+    from cmblensing_b200 import engine, matrix_operators as mo
+    from cmblensing_b200.simulate import ARCMIN, hole_mask, inference_problem
+    p = inference_problem(N, theta, beam_fwhm=1.0, noise_t=10.0, noise_p=2.0, seed=seed, bb_fraction=0.01)
+    pw = theta * ARCMIN
+    w = 2.0 * np.ones(N // 2 + 1, dtype=np.complex128)
+    w[0] = w[-1] = 1.0
+    kw = dict(nside=N, theta_pix=theta, pix_width=pw, fourier_weights=w)
+    mask = mo.PixelMask(mask_map=hole_mask(N, theta), **kw)
+    if C == 1:
+        f = cl.FlatS0(scalar_matrix=p["t"], **kw)
+        D = lambda a: mo.DiagonalScalar(scalar_matrix=a, **kw)
+        Cf, Cn, B, noise = D(p["cf_tt"]), D(p["cn_t"]), D(p["beam"]), [p["n_t"]]
+    else:
+        f = cl.FlatS2(polar_matrix_1=p["e"], polar_matrix_2=p["b"], **kw)
+        D = lambda a, b: mo.DiagonalEB(matrix_EE=a, matrix_BB=b, **kw)
+        Cf, Cn, B, noise = D(p["cf_ee"], p["cf_bb"]), D(p["cn_p"], p["cn_p"]), D(p["beam"], p["beam"]), [p["n_e"], p["n_b"]]
+    fmap = cl.map(cl.eb2qu(f))
+    mats = np.stack([getattr(fmap, k) for k in fmap._matrix_names()])[None]
+    lensed = engine.lense_flow_batch(torch.as_tensor(mats, device="cuda"),
+                                     torch.as_tensor(np.fft.irfft2(p["phi"], s=(N, N))[None], device="cuda"), pw,
+                                     n=7)[0].double().cpu().numpy()
+    lf = cl.qu2eb(cl.fourier(fmap.replace(**{k: lensed[i] for i, k in enumerate(fmap._matrix_names())})))
+    d = mask * (B * lf)
+    data = d.replace(**{k: getattr(d, k) + noise[i] for i, k in enumerate(d._matrix_names())})
+    return dict(phi=cl.FlatS0(scalar_matrix=p["phi"], **kw), data=data, Cf=Cf, Cn=Cn, M=mask, B=B)
+
+
+def run_serving(a):
+    """Config-4 stream: Poisson arrivals, mixed kinds/sizes/components; p50/p99 and throughput vs one at a time."""
+    import numpy as np
+    import torch
+    from cmblensing_b200.serve import Request, Server, latency_summary, run_alone
+    from cmblensing_b200.simulate import lens_batch
+    rng = np.random.default_rng(4242)
+    pools, wf = {}, {}
+    for N, th in SERVE_SIZES.items():
+        for C in (1, 2):
+            f, ph = lens_batch(N, th, 2, C, seed0=N + C)
+            pools[(N, C)] = (f, ph)
+            wf[(N, C)] = _wf_problem(N, C, th, seed=N + C)
+    wf_kw = dict(rel_tol=1e-5, refine_every=10, maxiter=300)
+
+    def make():
+        kind = rng.choice(["lens", "delens", "wf"], p=[0.5, 0.2, 0.3])
+        N = int(rng.choice(list(SERVE_SIZES), p=[0.4, 0.3, 0.2, 0.1]))
+        C = int(rng.choice([1, 2]))
+        th = SERVE_SIZES[N]
+        if kind == "wf":
+            return Request("wf", N, C, th, problem=wf[(N, C)], n=7, wf_kwargs=wf_kw)
+        f, ph = pools[(N, C)]
+        i = int(rng.integers(2))
+        return Request(str(kind), N, C, th, f=f[i], phi=ph[i], n=7)
+
+    # warm every shape once (graph capture, plans, kernel attributes) outside the measurement
+    srv = Server(max_batch=16, wf_workers=4).start()
+    warm = [srv.submit(Request(k, N, C, th, f=pools[(N, C)][0][0], phi=pools[(N, C)][1][0], n=7))
+            for N, th in SERVE_SIZES.items() for C in (1, 2) for k in ("lens", "delens")]
+    warm += [srv.submit(Request("wf", N, C, th, problem=wf[(N, C)], n=7, wf_kwargs=wf_kw))
+             for N, th in SERVE_SIZES.items() for C in (1, 2)]
+    for r in warm:
+        r.done.wait(300)
+    srv.completed.clear()
+    # the stream
+    nreq = int(rng.poisson(a.serving_rate * a.serving_seconds))
+    gaps = rng.exponential(1.0 / a.serving_rate, size=nreq)
+    reqs = [make() for _ in range(nreq)]
+    t0 = time.perf_counter()
+    tnext = t0
+    for r, g in zip(reqs, gaps):
+        tnext += g
+        dt = tnext - time.perf_counter()
+        if dt > 0:
+            time.sleep(dt)
+        srv.submit(r)
+    ok = all(r.done.wait(max(1.0, 600 - (time.perf_counter() - t0))) for r in reqs)
+    t_end = max((r.t_done for r in reqs if r.t_done), default=time.perf_counter())
+    srv.stop()
+    errors = sum(r.error is not None for r in reqs)
+    span = t_end - t0
+    out = {"requests": nreq, "arrival_rate_per_s": a.serving_rate, "seconds_of_arrivals": a.serving_seconds,
+           "all_completed": bool(ok), "errors": errors, "throughput_maps_per_s": nreq / span,
+           "latency": latency_summary(reqs),
+           "latency_by_kind": {k: latency_summary([r for r in reqs if r.kind == k]) for k in ("lens", "delens", "wf")},
+           "mix": "50% lens / 20% inverse / 30% Wiener filter; N 128/256/512/1024 at 0.4/0.3/0.2/0.1; T or QU 50/50"}
+    # one request at a time, plain engine calls, on a sample of the same mix
+    sample = reqs[: min(len(reqs), 40)]
+    torch.cuda.synchronize()
+    ts = time.perf_counter()
+    for r in sample:
+        run_alone(r)
+    torch.cuda.synchronize()
+    seq = (time.perf_counter() - ts) / max(len(sample), 1)
+    out["one_at_a_time"] = {"maps_per_s": 1.0 / seq, "sample_requests": len(sample)}
+    out["speedup_vs_one_at_a_time"] = out["throughput_maps_per_s"] * seq
+    return out
+
 # --------------------------------------------------------------------- main
 def main():
     a = parse()
@@ -385,6 +493,13 @@ def main():
                                       "what": "torch float64 restatement of the reference op sequence (cuFFT), "
                                               "not the reference", "speedup_of_value": value / world / (nb / dt),
                                       "rel_l2_fp32_vs_fp64": rel}
+
+    # ---------------------------------------------------- serving
+    if rank == 0 and a.serving_seconds > 0:
+        try:
+            result["serving"] = run_serving(a)
+        except Exception as e:  # the headline numbers stand on their own
+            result["serving"] = {"error": repr(e)}
 
     # ---------------------------------------------------- CPU baseline
     if pool is not None:

@@ -367,13 +367,37 @@ def get_plan(nside, ncomp, pix_width, precision="f32", device=None):
         return p
 
 
+_planes_cache = {}
+_PLANES_CACHE_SIZE = 8
+
+
+def cached_phi_planes(plan, phi, check_det=True):
+    """Derivative planes of ``phi`` for ``plan``, reused while the same phi tensor is unmodified.
+
+    The key is the tensor's storage pointer, shape, dtype and in-place version
+    counter, so repeated lensing by one phi (CG iterations, gradients) skips
+    the float64 precompute and the magnification-check readback.  The cache
+    holds a reference to the tensor, so its storage (and address) cannot be
+    reused by another tensor while the entry lives.
+    """
+    key = (id(plan), phi.data_ptr(), tuple(phi.shape), phi.dtype, phi._version)
+    hit = _planes_cache.get(key)
+    if hit is not None:
+        return hit[1]
+    planes = plan.phi_planes(phi, check_det=check_det)
+    if len(_planes_cache) >= _PLANES_CACHE_SIZE:
+        _planes_cache.pop(next(iter(_planes_cache)))
+    _planes_cache[key] = (phi, planes)
+    return planes
+
+
 def lense_flow_batch(f, phi, pix_width, n=10, direction=FORWARD_LENSE, adjoint=False, precision="f32",
                      check_det=True):
     """Batched LenseFlow on device tensors: f [B,C,N,N], phi [B,N,N] map or [B,N,N/2+1] Fourier."""
     if f.dim() == 3:
         f = f.unsqueeze(0)
     plan = get_plan(f.shape[-1], f.shape[1], pix_width, precision, device=f.device)
-    planes = plan.phi_planes(phi, check_det=check_det)
+    planes = cached_phi_planes(plan, phi, check_det=check_det)
     return plan.lense_flow(f, planes, n=n, direction=direction, adjoint=adjoint)
 
 

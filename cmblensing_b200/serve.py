@@ -10,7 +10,9 @@ its own stream, so batches of different shapes run concurrently on the
 device; while they run, newly arrived requests queue for the next batch of
 their group.  A batch's completion event frees its slot and memory and
 completes its requests.  Wiener-filter solves (data-dependent CG iteration
-counts) run eagerly on worker threads, each with its own stream.
+counts) run on worker threads, each with its own stream, with the
+device-resident PCG of ``wf_engine`` (operators precomputed per problem, CG
+scalars on the device).
 
 Each lensed map is computed by exactly the kernels and tiles it would use
 alone, so a request's result is bit-identical whether it runs alone or in a
@@ -280,7 +282,6 @@ class Server:
                 time.sleep(0.0002)
 
     def _wf_loop(self):
-        from .wiener_filter import wiener_filter
         torch.cuda.set_device(self.dev)
         stream = torch.cuda.Stream(self.dev)
         while True:
@@ -289,15 +290,24 @@ class Server:
                 return
             try:
                 with torch.cuda.stream(stream):
-                    P = r.problem
-                    r.result = wiener_filter(P["data"] * 0, P["phi"], P["data"], P["Cf"], P["Cn"], P["M"], P["B"],
-                                             n=r.n, **r.wf_kwargs)
+                    r.result = _solve_wf(r)
                     torch.cuda.current_stream().synchronize()
             except Exception as e:
                 r.error = e
             r.t_done = time.perf_counter()
             r.done.set()
             self._finish([r])
+
+
+def _solve_wf(req):
+    """One Wiener-filter request with the device-resident PCG; returns the host solution field."""
+    from .wf_engine import DeviceWienerFilter
+    P = req.problem
+    wf = DeviceWienerFilter(P["phi"], P["data"], P["Cf"], P["Cn"], P["M"], P["B"], n=req.n)
+    kw = dict(req.wf_kwargs)
+    x, it = wf.solve(**kw)
+    req.iterations = it
+    return wf.to_field(x)
 
 
 def nat_direction(kind):
@@ -307,10 +317,7 @@ def nat_direction(kind):
 def run_alone(req):
     """The same request executed by itself with plain engine calls (no batching, no graphs)."""
     if req.kind == "wf":
-        from .wiener_filter import wiener_filter
-        P = req.problem
-        return wiener_filter(P["data"] * 0, P["phi"], P["data"], P["Cf"], P["Cn"], P["M"], P["B"], n=req.n,
-                             **req.wf_kwargs)
+        return _solve_wf(req)
     plan = engine.get_plan(req.nside, req.ncomp, req.theta_pix * ARCMIN, "f32")
     f = torch.as_tensor(np.asarray(req.f, dtype=np.float32), device="cuda").unsqueeze(0)
     phi = torch.as_tensor(np.asarray(req.phi, dtype=np.float64), device="cuda").unsqueeze(0)
