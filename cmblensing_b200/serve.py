@@ -10,9 +10,10 @@ its own stream, so batches of different shapes run concurrently on the
 device; while they run, newly arrived requests queue for the next batch of
 their group.  A batch's completion event frees its slot and memory and
 completes its requests.  Wiener-filter solves (data-dependent CG iteration
-counts) run on worker threads, each with its own stream, with the
-device-resident PCG of ``wf_engine`` (operators precomputed per problem, CG
-scalars on the device).
+counts) wait per (N, components, pixel size); a free worker thread, each
+with its own stream, takes the oldest group (up to ``wf_batch`` problems)
+and solves it with the batched device-resident PCG of ``wf_engine``
+(operators precomputed per problem, CG scalars on the device).
 
 Each lensed map is computed by exactly the kernels and tiles it would use
 alone, so a request's result is bit-identical whether it runs alone or in a
@@ -172,7 +173,7 @@ class _LensSlot:
 class Server:
     """Continuous-batching scheduler over the LenseFlow engine on one GPU."""
 
-    def __init__(self, hbm_budget=32 << 30, max_batch=16, use_graphs=True, wf_workers=4, device=None):
+    def __init__(self, hbm_budget=32 << 30, max_batch=16, use_graphs=True, wf_workers=4, wf_batch=8, device=None):
         self.dev = torch.device("cuda", torch.cuda.current_device() if device is None else torch.device(device).index)
         self.budget = int(hbm_budget)
         self.max_batch = int(max_batch)
@@ -181,7 +182,10 @@ class Server:
         self.pending = collections.defaultdict(collections.deque)  # group key -> requests
         self.slots = {}  # group key -> list of _LensSlot
         self.in_use = 0
-        self.wf_queue = queue.Queue()
+        self.wf_batch = int(wf_batch)
+        self.wf_pending = collections.defaultdict(collections.deque)  # (N, C, theta) -> waiting WF requests
+        self.wf_cond = threading.Condition()
+        self._wf_stop = False
         self.completed = []
         self._stop = threading.Event()
         self._lock = threading.Lock()
@@ -203,8 +207,9 @@ class Server:
     def stop(self):
         self._stop.set()
         self._thread.join()
-        for _ in self._wf_threads:
-            self.wf_queue.put(None)
+        with self.wf_cond:
+            self._wf_stop = True
+            self.wf_cond.notify_all()
         for t in self._wf_threads:
             t.join()
 
@@ -255,7 +260,9 @@ class Server:
             while waiting and self._admit(waiting[0].footprint()):
                 r = waiting.popleft()
                 if r.kind == "wf":
-                    self.wf_queue.put(r)
+                    with self.wf_cond:
+                        self.wf_pending[(r.nside, r.ncomp, r.theta_pix)].append(r)
+                        self.wf_cond.notify()
                 else:
                     d = nat_direction(r.kind)
                     self.pending[(r.nside, r.ncomp, r.theta_pix, d)].append(r)
@@ -281,33 +288,58 @@ class Server:
             if not launched:
                 time.sleep(0.0002)
 
+    def _take_wf_batch(self):
+        """Block until Wiener-filter work is waiting; take up to wf_batch requests of the oldest group."""
+        with self.wf_cond:
+            while True:
+                groups = [(q[0].t_submit, k) for k, q in self.wf_pending.items() if q]
+                if groups:
+                    _, key = min(groups)
+                    q = self.wf_pending[key]
+                    return [q.popleft() for _ in range(min(len(q), self.wf_batch))]
+                if self._wf_stop:
+                    return None
+                self.wf_cond.wait(0.05)
+
     def _wf_loop(self):
         torch.cuda.set_device(self.dev)
         stream = torch.cuda.Stream(self.dev)
         while True:
-            r = self.wf_queue.get()
-            if r is None:
+            batch = self._take_wf_batch()
+            if batch is None:
                 return
             try:
                 with torch.cuda.stream(stream):
-                    r.result = _solve_wf(r)
+                    results = _solve_wf_batch(batch)
                     torch.cuda.current_stream().synchronize()
+                for r, x in zip(batch, results):
+                    r.result = x
             except Exception as e:
-                r.error = e
-            r.t_done = time.perf_counter()
-            r.done.set()
-            self._finish([r])
+                for r in batch:
+                    r.error = e
+            now = time.perf_counter()
+            for r in batch:
+                r.t_done = now
+                r.done.set()
+            self._finish(batch)
+
+
+def _solve_wf_batch(reqs):
+    """Wiener-filter requests of one (N, C, pixel size) solved together by the batched device PCG."""
+    from .wf_engine import DeviceWienerFilter
+    wf = DeviceWienerFilter(problems=[r.problem for r in reqs], n=reqs[0].n)
+    x, its = wf.solve(**reqs[0].wf_kwargs)
+    if len(reqs) == 1:
+        reqs[0].iterations = its
+        return [wf.to_field(x)]
+    for r, it in zip(reqs, its):
+        r.iterations = it
+    return [wf.to_field(x, i) for i in range(len(reqs))]
 
 
 def _solve_wf(req):
-    """One Wiener-filter request with the device-resident PCG; returns the host solution field."""
-    from .wf_engine import DeviceWienerFilter
-    P = req.problem
-    wf = DeviceWienerFilter(P["phi"], P["data"], P["Cf"], P["Cn"], P["M"], P["B"], n=req.n)
-    kw = dict(req.wf_kwargs)
-    x, it = wf.solve(**kw)
-    req.iterations = it
-    return wf.to_field(x)
+    """One Wiener-filter request by itself."""
+    return _solve_wf_batch([req])[0]
 
 
 def nat_direction(kind):

@@ -64,61 +64,98 @@ def _mm(A, B):
 
 
 class DeviceWienerFilter:
-    """The Wiener filter of one problem, with operators, phi planes and buffers resident on the GPU."""
+    """Wiener filters of a batch of problems (same N, components and pixel size), resident on the GPU.
 
-    def __init__(self, phi, data, field_covariance, noise_covariance, mask, beam, n=10, precision="f32"):
+    ``problems`` is a list of dicts with keys phi, data, Cf, Cn, M, B
+    (reference-shaped containers, host or device).  One application of A
+    lenses the whole batch in one engine launch sequence; the CG scalars are
+    per problem, and a problem that has converged keeps its iterate while the
+    others continue.  ``DeviceWienerFilter(phi, data, Cf, Cn, M, B)`` builds a
+    batch of one.
+    """
+
+    def __init__(self, phi=None, data=None, field_covariance=None, noise_covariance=None, mask=None, beam=None,
+                 n=10, precision="f32", problems=None):
+        if problems is None:
+            problems = [dict(phi=phi, data=data, Cf=field_covariance, Cn=noise_covariance, M=mask, B=beam)]
         dev = device()
         self.dev = dev
-        args = [to_device(o, dev) for o in (phi, data, field_covariance, noise_covariance, beam)]
-        phi, data, Cf, Cn, B = args
-        self.data = data
-        self.C = C = _ncomp(data)
-        self.N = N = data.nside
-        self.pw = data.pix_width
         self.n = n
         self.precision = precision
-        first = getattr(data, data._matrix_names()[0])
-        self.weights = torch.as_tensor(np.real(np.asarray(data.fourier_weights)), device=dev)
-        # rotation qu2eb per mode (identity on T)
-        R = torch.zeros((C, C, N, N // 2 + 1), dtype=torch.float64, device=dev)
-        if C == 1:
-            R[0, 0] = 1.0
-        else:
-            c2a, s2a = _eb_angle(N, data.theta_pix, first)
-            o = C - 2
-            if C == 3:
-                R[0, 0] = 1.0
-            R[o, o], R[o, o + 1] = -c2a, -s2a
-            R[o + 1, o], R[o + 1, o + 1] = s2a, -c2a
-        RT = R.transpose(0, 1).contiguous()
-        self.R, self.RT = R, RT
-        Cn_inv = _op_matrix(pinv(Cn), C, first)
-        Bm = _op_matrix(B, C, first)
-        self.Cf_inv = _op_matrix(pinv(Cf), C, first).to(torch.complex128)
+        self.batch = len(problems)
+        d0 = problems[0]["data"]
+        self.C = C = _ncomp(d0)
+        self.N = N = d0.nside
+        self.pw = d0.pix_width
+        self.theta = d0.theta_pix
+        self.datas, Rt, Wd, Bc, Cfi, Pinv, masks, Wb, Wn, bparts, phis, weights = [], [], [], [], [], [], [], [], [], [], [], []
+        for prob in problems:
+            phi_, data, Cf, Cn, B = [to_device(prob[k], dev) for k in ("phi", "data", "Cf", "Cn", "B")]
+            if (_ncomp(data), data.nside, data.theta_pix) != (C, N, self.theta):
+                raise ValueError("a batch of Wiener filters must share N, components and pixel size")
+            mask = prob["M"]
+            first = getattr(data, data._matrix_names()[0])
+            self.datas.append(data)
+            weights.append(torch.as_tensor(np.real(np.asarray(data.fourier_weights)), device=dev))
+            R = self._rotation(C, N, data.theta_pix, first)
+            RT = R.transpose(0, 1).contiguous()
+            Cn_inv = _op_matrix(pinv(Cn), C, first)
+            Bm = _op_matrix(B, C, first)
+            Cfi.append(_op_matrix(pinv(Cf), C, first))
+            if isinstance(mask, PixelMask):
+                masks.append(to_device(mask, dev).mask_map)
+                Mm = _op_matrix(mask.diagonal_like(B), C, first)
+                Wb.append(_mm(RT, _mm(Bm, R)))
+                Wn.append(_mm(RT, _mm(Cn_inv, R)))
+                bparts.append((_mm(RT, Cn_inv), _mm(Bm, R)))
+            else:
+                masks.append(None)
+                Mm = _op_matrix(mask, C, first)
+                Wd.append(_mm(RT, _mm(_mm(Bm, _mm(Mm, _mm(Cn_inv, _mm(Mm, Bm)))), R)))
+                Bc.append(_mm(Bm, _mm(Mm, Cn_inv)))
+            P = _op_matrix(pinv(Cf), C, first) + _mm(Bm, _mm(Mm, _mm(Cn_inv, _mm(Mm, Bm))))
+            Pinv.append(self._invert(P))
+            phis.append(to_map(phi_).scalar_matrix.to(torch.float64))
+        kinds = {m is None for m in masks}
+        if len(kinds) != 1:
+            raise ValueError("a batch mixes map-space and Fourier-diagonal masks")
+        cx = lambda lst: torch.stack(lst).to(torch.complex128)
+        self.R_c = R.to(torch.complex128)          # identical for the batch (same N, pixel size)
+        self.RT_c = RT.to(torch.complex128)
+        self.Cf_inv = cx(Cfi)
+        self.P_inv = cx(Pinv)
+        self.weights = torch.stack(weights)[:, None, None, :]  # (B, 1, 1, N/2+1)
         self.pixel_mask = None
-        if isinstance(mask, PixelMask):
-            self.pixel_mask = to_device(mask, dev).mask_map
-            mdiag = _op_matrix(mask.diagonal_like(B), C, first)
-            self.W_b = _mm(RT, _mm(Bm, R)).to(torch.complex128)          # QU -> QU through B
-            self.W_n = _mm(RT, _mm(Cn_inv, R)).to(torch.complex128)      # QU -> QU through Cn^-1
-            self._b_parts = (_mm(RT, Cn_inv).to(torch.complex128), _mm(Bm, R).to(torch.complex128))
-            Mm = mdiag
+        if masks[0] is not None:
+            self.pixel_mask = torch.stack(masks)[:, None]         # (B, 1, N, N)
+            self.W_b, self.W_n = cx(Wb), cx(Wn)
+            self._b_rt_cn = cx([b[0] for b in bparts])
+            self._b_bm_r = cx([b[1] for b in bparts])
         else:
-            Mm = _op_matrix(mask, C, first)
-            data_op = _mm(Bm, _mm(Mm, _mm(Cn_inv, _mm(Mm, Bm))))
-            self.W_data = _mm(RT, _mm(data_op, R)).to(torch.complex128)   # QU -> QU
-            self._bm_cn = _mm(Bm, _mm(Mm, Cn_inv)).to(torch.complex128)    # EB -> EB, for b
-        P = _op_matrix(pinv(Cf), C, first) + _mm(Bm, _mm(Mm, _mm(Cn_inv, _mm(Mm, Bm))))
-        self.P_inv = self._invert(P).to(torch.complex128)
-        self.R_c, self.RT_c = R.to(torch.complex128), RT.to(torch.complex128)
-        phimap = to_map(phi).scalar_matrix.to(torch.float64).unsqueeze(0)  # gradients.py:17 uses map(phi)
-        self.phimap = phimap
+            self.W_data, self._bm_cn = cx(Wd), cx(Bc)
+        self.d = torch.stack([torch.stack([getattr(dd, k) for k in dd._matrix_names()]) for dd in self.datas])
+        self.phimap = torch.stack(phis)
         self.plan = engine.get_plan(N, C, self.pw, precision, device=dev)
-        self.planes = engine.cached_phi_planes(self.plan, phimap)
+        self.planes = engine.cached_phi_planes(self.plan, self.phimap)
         self.fft = engine.get_plan(N, 1, self.pw, "f64", device=dev)
         self._plan64 = None
 
     # ----------------------------------------------------------- pieces
+    @staticmethod
+    def _rotation(C, N, theta, like):
+        """Per-mode qu2eb rotation (util.py:152-161), identity on T."""
+        R = torch.zeros((C, C, N, N // 2 + 1), dtype=torch.float64, device=like.device)
+        if C == 1:
+            R[0, 0] = 1.0
+            return R
+        c2a, s2a = _eb_angle(N, theta, like)
+        o = C - 2
+        if C == 3:
+            R[0, 0] = 1.0
+        R[o, o], R[o, o + 1] = -c2a, -s2a
+        R[o + 1, o], R[o + 1, o + 1] = s2a, -c2a
+        return R
+
     @staticmethod
     def _invert(P):
         """Per-mode pseudo-inverse of a block-diagonal C x C matrix (reciprocal with 0 -> 0, Schur for TE)."""
@@ -132,20 +169,25 @@ class DeviceWienerFilter:
         else:  # [TT TE 0; ET EE 0; 0 0 BB] as matrix_operators.py:222-234
             a, b, c, d = P[0, 0], P[0, 1], P[1, 0], P[1, 1]
             rd = rec(d)
-            s = rec(a - b * rd * c)
-            out[0, 0], out[0, 1], out[1, 0], out[1, 1] = s, -s * b * rd, -rd * c * s, rd + rd * c * s * b * rd
+            sc = rec(a - b * rd * c)
+            out[0, 0], out[0, 1], out[1, 0], out[1, 1] = sc, -sc * b * rd, -rd * c * sc, rd + rd * c * sc * b * rd
             out[2, 2] = rec(P[2, 2])
         return out
 
     @staticmethod
     def _apply(W, X):
-        return torch.einsum("ijnh,jnh->inh", W, X)
+        """Per-mode matrix times vector: W (C,C,N,H) shared or (B,C,C,N,H) per problem; X (B,C,N,H)."""
+        if W.dim() == 4:
+            return torch.einsum("ijnh,bjnh->binh", W, X)
+        return torch.einsum("bijnh,bjnh->binh", W, X)
 
     def _irfft2(self, X):
-        return self.fft.irfft2(X)
+        B, C = X.shape[:2]
+        return self.fft.irfft2(X.reshape(B * C, self.N, self.N // 2 + 1)).reshape(B, C, self.N, self.N)
 
     def _rfft2(self, X):
-        return self.fft.rfft2(X)
+        B, C = X.shape[:2]
+        return self.fft.rfft2(X.reshape(B * C, self.N, self.N)).reshape(B, C, self.N, self.N // 2 + 1)
 
     def _lens(self, q, adjoint, prec):
         if prec == self.precision:
@@ -155,7 +197,7 @@ class DeviceWienerFilter:
                 self._plan64 = engine.get_plan(self.N, self.C, self.pw, prec, device=self.dev)
                 self._planes64 = engine.cached_phi_planes(self._plan64, self.phimap)
             plan, planes = self._plan64, self._planes64
-        return plan.lense_flow(q.unsqueeze(0), planes, n=self.n, adjoint=adjoint)[0]
+        return plan.lense_flow(q, planes, n=self.n, adjoint=adjoint)
 
     def _mask_chain(self, y):
         """QU spectra -> W y through the map-space mask: B, m, Cn^-1, m, B."""
@@ -167,68 +209,80 @@ class DeviceWienerFilter:
         return self._apply(self.W_b, t)
 
     def apply_A(self, x, prec=None):
-        """A x = gradf_logpdf(x, d = 0) for an EB/T spectrum x of shape (C, N, N/2+1)."""
+        """A x = gradf_logpdf(x, d = 0) for EB/T spectra x of shape (B, C, N, N/2+1) (or (C, N, N/2+1))."""
+        single = x.dim() == 3
+        if single:
+            x = x.unsqueeze(0)
         prec = prec or self.precision
         y = self._rfft2(self._lens(self._irfft2(self._apply(self.RT_c, x)), False, prec))
         h = self._mask_chain(y) if self.pixel_mask is not None else self._apply(self.W_data, y)
         z = self._rfft2(self._lens(self._irfft2(h), True, prec))
-        return -(self._apply(self.R_c, z) + self._apply(self.Cf_inv, x))
+        out = -(self._apply(self.R_c, z) + self._apply(self.Cf_inv, x))
+        return out[0] if single else out
 
     def b_vector(self, prec=None):
-        """b = -gradf_logpdf(0, d) (wiener_filter.py:29-33)."""
+        """b = -gradf_logpdf(0, d) (wiener_filter.py:29-33), (B, C, N, N/2+1)."""
         prec = prec or self.precision
-        d = torch.stack([getattr(self.data, k) for k in self.data._matrix_names()])
         if self.pixel_mask is not None:
-            rt_cn, bm_r = self._b_parts
-            t = self._rfft2(self._irfft2(self._apply(rt_cn, d)) * self.pixel_mask)  # QU after Cn^-1 and m
-            v = self._apply(bm_r, t)                                               # EB after B
-            h = self._apply(self.RT_c, v)
+            t = self._rfft2(self._irfft2(self._apply(self._b_rt_cn, self.d)) * self.pixel_mask)
+            h = self._apply(self.RT_c, self._apply(self._b_bm_r, t))
         else:
-            h = self._apply(self.RT_c, self._apply(self._bm_cn, d))
+            h = self._apply(self.RT_c, self._apply(self._bm_cn, self.d))
         z = self._rfft2(self._lens(self._irfft2(h), True, prec))
         return -self._apply(self.R_c, z)
 
     def dot(self, a, b):
-        """fields.dot: Re sum conj(a) b w / N^2, float64, as a device scalar."""
-        return torch.real(torch.sum(torch.conj(a) * b * self.weights)) / (self.N * self.N)
+        """fields.dot per problem: Re sum conj(a) b w / N^2, float64 device tensor of shape (B,)."""
+        return torch.real(torch.sum(torch.conj(a) * b * self.weights, dim=(1, 2, 3))) / (self.N * self.N)
 
     # ------------------------------------------------------------ solve
     def solve(self, x0=None, rel_tol=None, tol=1e-1, maxiter=500, refine_every=0, check_every=1, history=None):
-        """PCG with the reference recurrence; returns (x, iterations).  Stopping as wiener_filter.py:75-77
+        """PCG with the reference recurrence for every problem; returns (x, iterations) for a batch of one,
+        else (x [B, C, N, N/2+1], iterations per problem).  Stopping per problem as wiener_filter.py:75-77
         (r.z < tol) unless ``rel_tol`` is given (||r|| / ||b||)."""
         b = self.b_vector()
-        x = torch.zeros_like(b) if x0 is None else x0
+        x = torch.zeros_like(b) if x0 is None else (x0 if x0.dim() == 4 else x0.unsqueeze(0))
         r = b - self.apply_A(x) if x0 is not None else b.clone()
         z = self._apply(self.P_inv, r)
         p = z.clone()
         res = self.dot(r, z)
         bnorm = torch.sqrt(self.dot(b, b))
+        active = torch.ones(self.batch, dtype=torch.bool, device=self.dev)
+        iters = torch.zeros(self.batch, dtype=torch.int64, device=self.dev)
         it = 0
+        bc = lambda v: v[:, None, None, None]
         while it < maxiter:
             if it % check_every == 0:
                 if rel_tol is None:
-                    if not float(res) >= tol:
-                        break
+                    active = active & (res >= tol)
                 else:
-                    rn = float(torch.sqrt(torch.clamp(self.dot(r, r), min=0.0)) / bnorm)
+                    rn = torch.sqrt(torch.clamp(self.dot(r, r), min=0.0)) / bnorm
                     if history is not None:
-                        history.append(rn)
-                    if rn < rel_tol:
-                        break
+                        history.append(rn.cpu().numpy())
+                    active = active & ~(rn < rel_tol)
+                if not bool(active.any()):
+                    break
             Ap = self.apply_A(p)
-            alpha = res / self.dot(p, Ap)
-            x = x + alpha * p
+            pAp = self.dot(p, Ap)
+            alpha = torch.where(active, res / torch.where(pAp != 0, pAp, torch.ones_like(pAp)), torch.zeros_like(res))
+            x = x + bc(alpha) * p
+            iters = iters + active.to(torch.int64)
             it += 1
             if refine_every and it % refine_every == 0:
-                r = b - self.apply_A(x, "f64")
+                r = torch.where(bc(active), b - self.apply_A(x, "f64"), r)
             else:
-                r = r - alpha * Ap
+                r = r - bc(alpha) * Ap
             z = self._apply(self.P_inv, r)
             res_new = self.dot(r, z)
-            p = z + (res_new / res) * p
-            res = res_new
-        return x, it
+            beta = torch.where(active, res_new / torch.where(res != 0, res, torch.ones_like(res)), torch.zeros_like(res))
+            p = z + bc(beta) * p
+            res = torch.where(active, res_new, res)
+        if self.batch == 1:
+            return x[0], int(iters[0])
+        return x, iters.cpu().tolist()
 
-    def to_field(self, x):
-        """The solution as a reference-shaped field on the host."""
-        return self.data.replace(**{k: x[i].cpu().numpy() for i, k in enumerate(self.data._matrix_names())})
+    def to_field(self, x, i=0):
+        """Solution ``i`` (or the only one) as a reference-shaped field on the host."""
+        xi = x if x.dim() == 3 else x[i]
+        data = self.datas[i]
+        return data.replace(**{k: xi[j].cpu().numpy() for j, k in enumerate(data._matrix_names())})

@@ -229,3 +229,27 @@ def test_device_wiener_filter_matches_reference_shaped_solver(torch_cuda, masked
     g = gradf_logpdf(xf, S["phi"], xf * 0, S["Cf"], S["Cn"], S["M"], S["B"], n=7)
     for i, k in enumerate(g._matrix_names()):  # same kernels; the EB->QU sums round differently before FP32
         assert rel_l2(Ax[i].cpu().numpy(), getattr(g, k)) < 1e-6
+
+
+def test_batched_wiener_filter_equals_solo_solves(torch_cuda):
+    """Three masked problems of one size solved together by the batched CG equal their solo solves."""
+    import cmblensing_b200 as cl
+    from cmblensing_b200 import matrix_operators as mo
+    from cmblensing_b200.simulate import hole_mask
+    from cmblensing_b200.wf_engine import DeviceWienerFilter
+
+    class Mod:
+        FlatS0, FlatS2, FlatS02 = cl.FlatS0, cl.FlatS2, cl.FlatS02
+        DiagonalScalar, DiagonalEB, BlockTEB = mo.DiagonalScalar, mo.DiagonalEB, mo.BlockTEB
+
+    probs = []
+    for seed in (11, 12, 13):
+        S = _problem(Mod, 128, 2.0, "P", 1.0, 2.0, 2.0, seed=seed, bb_fraction=0.01,
+                     mask=hole_mask(128, 2.0, nholes=5, seed=seed))
+        probs.append(dict(phi=S["phi"], data=S["data"], Cf=S["Cf"], Cn=S["Cn"], M=S["M"], B=S["B"]))
+    batch = DeviceWienerFilter(problems=probs, n=7)
+    xb, its = batch.solve(rel_tol=1e-9, refine_every=10)
+    for i, pr in enumerate(probs):
+        solo = DeviceWienerFilter(problems=[pr], n=7)
+        xs, _ = solo.solve(rel_tol=1e-9, refine_every=10)
+        assert rel_l2(xb[i].cpu().numpy(), xs.cpu().numpy()) < 1e-7, (i, its)

@@ -2,8 +2,10 @@
 
 Lens and delens requests are batched and replayed from captured CUDA graphs;
 each map still runs the kernels and tiles it would use alone, so results
-must be bit-identical.  Wiener-filter solves run on worker streams and must
-equal a solo solve to 1e-12 relative (same kernels, same reductions).
+must be bit-identical.  Wiener-filter requests of one size are solved
+together by the batched CG, whose inner products sum in a different order
+than a solo solve: they must agree with the solo solution within the
+workload's CG tolerance, 1e-6.
 """
 import threading
 import time
@@ -57,7 +59,7 @@ def test_mixed_stream_equals_solo_runs(torch_cuda):
         C = [1, 2][rng.integers(2)]
         kind = ["lens", "delens"][rng.integers(2)]
         reqs.append(_lens_req(kind, N, C, 3.0 if N < 256 else 2.0, seed=10 * i))
-    reqs += [_wf_req(64, seed=s) for s in (1, 2)]
+    reqs += [_wf_req(64, seed=s) for s in (1, 2, 3)]
     srv = Server(max_batch=8, wf_workers=2).start()
     for r in reqs:
         srv.submit(r)
@@ -70,7 +72,7 @@ def test_mixed_stream_equals_solo_runs(torch_cuda):
         alone = run_alone(r)
         if r.kind == "wf":
             for k in alone._matrix_names():
-                assert rel_l2(getattr(r.result, k), getattr(alone, k)) < 1e-12
+                assert rel_l2(getattr(r.result, k), getattr(alone, k)) < 1e-6
         else:
             assert np.array_equal(r.result, alone), (r.kind, r.nside, r.ncomp)
     s = latency_summary(reqs)
