@@ -197,6 +197,22 @@ class ClockSampler:
         return {"sm_mhz": med, "sm_max_mhz": mx, "reasons": sorted(reasons), "samples": len(sm)}
 
 
+# ------------------------------------------------------------ multi-rank
+def max_over_ranks(ms, dist=None, device="cpu"):
+    """The slowest rank's time (every rank must call this, in the same order)."""
+    if dist is None:
+        return float(ms)
+    import torch
+    t = torch.tensor([float(ms)], dtype=torch.float64, device=device)
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
+
+
+def aggregate_value(world, batch_per_rank, steps, ms):
+    """Whole-job maps/s: every rank lenses its own batch; the job takes the slowest rank's time."""
+    return world * batch_per_rank * steps / (ms / 1000.0)
+
+
 # ----------------------------------------------------------- algorithmic bytes
 def row_bytes_per_lens(C, n, P, in_bytes=4, out_bytes=4):
     """Bytes the row kernels of one forward lens must move per map (float32 state, 5 phi planes).
@@ -407,11 +423,8 @@ def main():
     row_ms, row_n = plan.profile_read(nat.LF_KIND_ROW)
     col_ms, col_n = plan.profile_read(nat.LF_KIND_COL)
     phi_ms, phi_n = plan.profile_read(nat.LF_KIND_PHI)
-    if dist is not None:
-        t = torch.tensor([ms], device=dev)
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        ms = float(t.item())
-    value = world * B * a.steps / (ms / 1000.0)
+    ms = max_over_ranks(ms, dist, dev)
+    value = aggregate_value(world, B, a.steps, ms)
 
     # parity spot check of this run's output (one map) against the first lens of the batch in FP64 engine
     peaks = {}
@@ -462,12 +475,8 @@ def main():
             pipe(fh, ph, oh, n=n)
         e1.record()
         barrier()
-        ems = e0.elapsed_time(e1)
-        if dist is not None:
-            t = torch.tensor([ems], device=dev)
-            dist.all_reduce(t, op=dist.ReduceOp.MAX)
-            ems = float(t.item())
-        result["e2e"] = {"value": world * B * a.steps / (ems / 1000.0), "unit": UNIT,
+        ems = max_over_ranks(e0.elapsed_time(e1), dist, dev)
+        result["e2e"] = {"value": aggregate_value(world, B, a.steps, ems), "unit": UNIT,
                          "h2d_bytes_per_step": pipe.h2d_bytes(), "d2h_bytes_per_step": pipe.d2h_bytes(),
                          "api": "engine.HostPipeline (float64 host I/O, pinned)"}
         # parity of the bench output against the device-resident leg
