@@ -147,11 +147,18 @@ template <typename T, int LINES> __device__ __forceinline__ int sw(int m, int li
 }
 
 // ------------------------------------------------------------ Stockham pass
-// One radix-R pass over NLINES lines (line l lives in tile (l / LINES) of a
-// sequence of tiles spaced TILE_ELEMS apart) of length L.  NS is the
-// product of the radices of the previous passes.  ``tw`` holds NTAB entries.
-template <typename T, int L, int R, int NS, int LINES, int NTILES, int NT, bool INV, int NTAB>
-__device__ __forceinline__ void stockham_pass(c2<T>* __restrict__ buf, const c2<T>* __restrict__ tw, int tid) {
+// One radix-R pass over the LINES lines of NTILES consecutive tiles
+// (TILE_ELEMS apart) of length L.  NS is the product of the radices of the
+// previous passes.  ``tw`` holds NTAB entries.  ``pre(m, line, v)`` may
+// transform each input element as it is loaded (used to fold a spectral
+// multiplier into the first pass of a transform).
+struct NoPre {
+  template <typename V> __device__ __forceinline__ V operator()(int, int, int, V v) const { return v; }
+};
+
+template <typename T, int L, int R, int NS, int LINES, int NTILES, int NT, bool INV, int NTAB, class Pre = NoPre>
+__device__ __forceinline__ void stockham_pass(c2<T>* __restrict__ buf, const c2<T>* __restrict__ tw, int tid,
+                                              Pre pre = Pre()) {
   constexpr int NB = L / R;                   // butterflies per line
   constexpr int TOT = NB * LINES * NTILES;    // butterflies in the pass
   constexpr int PER = (TOT + NT - 1) / NT;
@@ -169,7 +176,7 @@ __device__ __forceinline__ void stockham_pass(c2<T>* __restrict__ buf, const c2<
       const int tile = rest / NB;
       const c2<T>* tb = buf + tile * TILE_ELEMS;
 #pragma unroll
-      for (int r = 0; r < R; ++r) v[b][r] = tb[sw<T, LINES>(j + r * NB, line)];
+      for (int r = 0; r < R; ++r) v[b][r] = pre(tile, j + r * NB, line, tb[sw<T, LINES>(j + r * NB, line)]);
       if constexpr (NS > 1) {
         const int k = j % NS;
 #pragma unroll
@@ -197,28 +204,29 @@ __device__ __forceinline__ void stockham_pass(c2<T>* __restrict__ buf, const c2<
   __syncthreads();
 }
 
-// Full transform of length L on NTILES consecutive tiles (LINES lines each).
+// Full transform of length L on NTILES consecutive tiles (LINES lines each);
+// ``pre`` is applied to the elements as the first pass loads them.
 // Radix plans: 32 = 8x4, 64 = 8x8, 128 = 8x16, 256 = 16x16, 512 = 8x8x8, 1024 = 16x8x8.
-template <typename T, int L, int LINES, int NTILES, int NT, bool INV, int NTAB>
-__device__ __forceinline__ void fft_tiles(c2<T>* buf, const c2<T>* tw, int tid) {
+template <typename T, int L, int LINES, int NTILES, int NT, bool INV, int NTAB, class Pre = NoPre>
+__device__ __forceinline__ void fft_tiles(c2<T>* buf, const c2<T>* tw, int tid, Pre pre = Pre()) {
   if constexpr (L == 32) {
-    stockham_pass<T, L, 8, 1, LINES, NTILES, NT, INV, NTAB>(buf, tw, tid);
+    stockham_pass<T, L, 8, 1, LINES, NTILES, NT, INV, NTAB>(buf, tw, tid, pre);
     stockham_pass<T, L, 4, 8, LINES, NTILES, NT, INV, NTAB>(buf, tw, tid);
   } else if constexpr (L == 64) {
-    stockham_pass<T, L, 8, 1, LINES, NTILES, NT, INV, NTAB>(buf, tw, tid);
+    stockham_pass<T, L, 8, 1, LINES, NTILES, NT, INV, NTAB>(buf, tw, tid, pre);
     stockham_pass<T, L, 8, 8, LINES, NTILES, NT, INV, NTAB>(buf, tw, tid);
   } else if constexpr (L == 128) {
-    stockham_pass<T, L, 8, 1, LINES, NTILES, NT, INV, NTAB>(buf, tw, tid);
+    stockham_pass<T, L, 8, 1, LINES, NTILES, NT, INV, NTAB>(buf, tw, tid, pre);
     stockham_pass<T, L, 16, 8, LINES, NTILES, NT, INV, NTAB>(buf, tw, tid);
   } else if constexpr (L == 256) {
-    stockham_pass<T, L, 16, 1, LINES, NTILES, NT, INV, NTAB>(buf, tw, tid);
+    stockham_pass<T, L, 16, 1, LINES, NTILES, NT, INV, NTAB>(buf, tw, tid, pre);
     stockham_pass<T, L, 16, 16, LINES, NTILES, NT, INV, NTAB>(buf, tw, tid);
   } else if constexpr (L == 512) {
-    stockham_pass<T, L, 8, 1, LINES, NTILES, NT, INV, NTAB>(buf, tw, tid);
+    stockham_pass<T, L, 8, 1, LINES, NTILES, NT, INV, NTAB>(buf, tw, tid, pre);
     stockham_pass<T, L, 8, 8, LINES, NTILES, NT, INV, NTAB>(buf, tw, tid);
     stockham_pass<T, L, 8, 64, LINES, NTILES, NT, INV, NTAB>(buf, tw, tid);
   } else if constexpr (L == 1024) {
-    stockham_pass<T, L, 16, 1, LINES, NTILES, NT, INV, NTAB>(buf, tw, tid);
+    stockham_pass<T, L, 16, 1, LINES, NTILES, NT, INV, NTAB>(buf, tw, tid, pre);
     stockham_pass<T, L, 8, 16, LINES, NTILES, NT, INV, NTAB>(buf, tw, tid);
     stockham_pass<T, L, 8, 128, LINES, NTILES, NT, INV, NTAB>(buf, tw, tid);
   } else {
@@ -263,21 +271,25 @@ __device__ __forceinline__ void r2c_post(c2<T>* buf, const c2<T>* twN, int tid) 
 // Before an inverse length-H FFT: turn the packed spectrum X into Z, in place,
 // so that IFFT_H(Z) = unnormalised inverse real DFT of X (x[2m] + i x[2m+1]).
 // The imaginary parts of X[0] and X[H] are never used, exactly as irfft does.
-template <typename T, int H, int LINES, int NTILES, int NT>
-__device__ __forceinline__ void c2r_pre(c2<T>* buf, const c2<T>* twN, int tid) {
+// ``in(tile, k, line, x)`` may transform each packed input element X[k] as it
+// is read (k = 0 is the (X0, XH) slot); it lets callers fold a spectral
+// multiplier into this pass.
+template <typename T, int H, int LINES, int NTILES, int NT, class In = NoPre>
+__device__ __forceinline__ void c2r_pre(c2<T>* buf, const c2<T>* twN, int tid, In in = In()) {
   constexpr int ITEMS = (H / 2 + 1) * LINES * NTILES;
   constexpr int TILE_ELEMS = H * LINES;
   for (int idx = tid; idx < ITEMS; idx += NT) {
     const int line = idx % LINES;
     const int rest = idx / LINES;
     const int k = rest % (H / 2 + 1);
-    c2<T>* tb = buf + (rest / (H / 2 + 1)) * TILE_ELEMS;
+    const int tile = rest / (H / 2 + 1);
+    c2<T>* tb = buf + tile * TILE_ELEMS;
     if (k == 0) {
-      c2<T> x = tb[sw<T, LINES>(0, line)];  // (X0, XH)
+      c2<T> x = in(tile, 0, line, tb[sw<T, LINES>(0, line)]);  // (X0, XH)
       tb[sw<T, LINES>(0, line)] = mk<T>(x.x + x.y, x.x - x.y);
     } else {
-      const c2<T> a = tb[sw<T, LINES>(k, line)];
-      const c2<T> bc = cconj<T>(tb[sw<T, LINES>(H - k, line)]);
+      const c2<T> a = in(tile, k, line, tb[sw<T, LINES>(k, line)]);
+      const c2<T> bc = cconj<T>(in(tile, H - k, line, tb[sw<T, LINES>(H - k, line)]));
       const c2<T> p = cadd<T>(a, bc);
       // q = i * W^{-k} (a - bc), W^{-k} = conj(twN[k])
       const c2<T> q = cmul_i<T>(cmulc<T>(csub<T>(a, bc), twN[k]));

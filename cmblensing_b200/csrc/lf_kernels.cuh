@@ -126,17 +126,15 @@ __global__ void __launch_bounds__(NT, MINB) k_col(StageArgs a) {
   load_cols<T, N, LINES, NT>(buf, in, H, c0, H, tid);
   __syncthreads();
   fft_tiles<T, N, LINES, 1, NT, false, N>(buf, tw, tid);
+  // i KX / N^2, folded into the first inverse pass; zero on KX's Nyquist row of
+  // the packed DC/Nyquist line (column 0)
   const T scale = T(a.kbase / (double(N) * double(N)));
-  for (int idx = tid; idx < N * LINES; idx += NT) {
-    const int m = idx / LINES, line = idx % LINES;
+  auto kx_mul = [=](int, int m, int line, c2<T> v) {
     const int kx = (m < N / 2) ? m : m - N;
-    T f = scale * T(kx);
-    if (c0 + line == 0 && m == N / 2) f = T(0);  // packed DC/Nyquist line
-    const c2<T> v = buf[sw<T, LINES>(m, line)];
-    buf[sw<T, LINES>(m, line)] = mk<T>(-f * v.y, f * v.x);
-  }
-  __syncthreads();
-  fft_tiles<T, N, LINES, 1, NT, true, N>(buf, tw, tid);
+    const T f = (c0 + line == 0 && m == N / 2) ? T(0) : scale * T(kx);
+    return mk<T>(-f * v.y, f * v.x);
+  };
+  fft_tiles<T, N, LINES, 1, NT, true, N>(buf, tw, tid, kx_mul);
   store_cols<T, N, LINES, NT>(out, H, c0, H, buf, tid);
 }
 
@@ -187,25 +185,24 @@ __global__ void __launch_bounds__(NT, MINB) k_row(StageArgs a) {
       load_rows<T, c2<T>, H, LINES, NT>(buf + (C + c) * TILE, spec(ADJ ? a.v : a.s, c), H, tid);
     }
     __syncthreads();
-    // d_y in the row spectrum: i KY / N (KY's DC and Nyquist bins contribute
-    // nothing after the inverse real transform)
-    for (int idx = tid; idx < H * LINES * C; idx += NT) {
-      const int c = idx / (H * LINES), rem = idx % (H * LINES);
-      const int row = rem / H, kk = rem % H;
-      c2<T>* sec = buf + (C + c) * TILE;
-      const c2<T> w = sec[sw<T, LINES>(kk, row)];
+    // d_y in the row spectrum: i KY / N, folded into the pre-pass of the
+    // inverse real transform (KY's DC and Nyquist bins contribute nothing
+    // after it, so the (X0, XH) slot of a d_y spectrum is zero).
+    auto dy = [=](const c2<T> w, int kk) {
       const T f = ky_scale * T(kk);
-      const c2<T> dy = (kk == 0) ? mk<T>(T(0), T(0)) : mk<T>(-f * w.y, f * w.x);
-      if constexpr (ADJ) {
-        c2<T>* pri = buf + c * TILE;
-        if (kk != 0) pri[sw<T, LINES>(kk, row)] = cadd<T>(pri[sw<T, LINES>(kk, row)], dy);
-      } else {
-        sec[sw<T, LINES>(kk, row)] = dy;
-      }
-    }
-    __syncthreads();
+      return (kk == 0) ? mk<T>(T(0), T(0)) : mk<T>(-f * w.y, f * w.x);
+    };
     constexpr int NTI = ADJ ? C : 2 * C;
-    c2r_pre<T, H, LINES, NTI, NT>(buf, tw, tid);
+    if constexpr (ADJ) {
+      // primary = Gx + i KY V / N: one inverse transform per component
+      auto in = [=](int tile, int kk, int row, c2<T> g) {
+        return (kk == 0) ? g : cadd<T>(g, dy(buf[(C + tile) * TILE + sw<T, LINES>(kk, row)], kk));
+      };
+      c2r_pre<T, H, LINES, NTI, NT>(buf, tw, tid, in);
+    } else {
+      auto in = [=](int tile, int kk, int, c2<T> w) { return tile < C ? w : dy(w, kk); };
+      c2r_pre<T, H, LINES, NTI, NT>(buf, tw, tid, in);
+    }
     fft_tiles<T, H, LINES, NTI, NT, true, N>(buf, tw, tid);
   } else {
     for (int idx = tid; idx < H * LINES * C; idx += NT) {
