@@ -59,9 +59,17 @@ def on_device(fn):
         for a in args:
             conv.append(to_device(a, dev) if hasattr(a, "_matrix_names") else a)
         out = fn(*conv, **kwargs)
-        if host and hasattr(out, "_matrix_names"):
-            return to_host(out)
-        if host and isinstance(out, torch.Tensor):
-            return float(out) if out.dim() == 0 else out.cpu().numpy()
-        return out
+        if not host:
+            return out
+        if isinstance(out, tuple):
+            return tuple(_host_result(o) for o in out)
+        return _host_result(out)
     return wrapper
+
+
+def _host_result(out):
+    if hasattr(out, "_matrix_names"):
+        return to_host(out)
+    if isinstance(out, torch.Tensor):
+        return float(out) if out.dim() == 0 else out.cpu().numpy()
+    return out

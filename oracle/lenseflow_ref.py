@@ -668,6 +668,51 @@ def grad_phi_logpdf(field, phi, data, noise_covariance, phi_covariance, field_co
     return dphi.scalar_matrix - prior.scalar_matrix
 
 
+# ------------------------------------------------------------------ mixing
+def mix(field, phi, mixing_d, mixing_g, n=10):
+    """mixing.py:8-20: f_mixed = qu2eb(fourier(L(phi) map(eb2qu(D f)))), phi_mixed = G phi."""
+    df = map_(eb2qu(mixing_d * field))
+    mixed_field = qu2eb(fourier(lense_flow(df, map_(phi), n=n)))
+    return mixed_field, mixing_g * phi
+
+
+def unmix(mixed_field, mixed_phi, mixing_d, mixing_g, n=10):
+    """mixing.py:23-36: phi = G^-1 phi_mixed, f = D^-1 qu2eb(fourier(L^-1(phi) map(eb2qu(f_mixed))))."""
+    phi = pinv(mixing_g) * mixed_phi
+    mmap = map_(eb2qu(mixed_field))
+    field = qu2eb(fourier(lense_flow(mmap, map_(phi), n=n, direction=INVERSE_LENSE)))
+    return pinv(mixing_d) * field, phi
+
+
+def mixing_jacobian_phi_component(mixed_field, phi, grad_f, mixing_d, n=10):
+    """gradients.py:63-85: the pullback of phi -> map(D^-1 qu2eb(fourier(L^-1(phi) f_mixed_map))).
+
+    phi is Fourier-shaped, so the reference's custom VJP returns delta-phi in
+    the Fourier basis.  The pullback of ``map`` applied to the cotangent
+    map(grad_f) is w conj(rfft2(map(grad_f))) / N^2 (JAX's irfft2 transpose),
+    D^-1 and qu2eb transpose to themselves / eb2qu (real coefficients per
+    mode), and the transpose of ``fourier`` is N^2 irfft2(conj(.) / w).  The
+    weights and conjugations cancel, so the cotangent of the inverse-lensed QU
+    map is map(eb2qu(D^-1 fourier(map(grad_f)))).
+    """
+    mmap = map_(eb2qu(mixed_field))
+    unlensed = lense_flow(mmap, phi, n=n, direction=INVERSE_LENSE)
+    cot = map_(eb2qu(pinv(mixing_d) * fourier(map_(grad_f))))
+    _, dphi = lense_flow_backwards(unlensed, phi, cot, n=n, direction=INVERSE_LENSE)
+    return dphi.scalar_matrix
+
+
+def mixed_grad_phi_logpdf(mixed_field, mixed_phi, data, noise_covariance, phi_covariance, field_covariance,
+                          mask, beam, mixing_d, mixing_g, n=10):
+    """gradients.py:41-60: G^-1 (grad_phi logpdf + J_phi^T grad_f logpdf) at the unmixed point."""
+    field, phi = unmix(mixed_field, mixed_phi, mixing_d, mixing_g, n=n)
+    grad_phi = grad_phi_logpdf(field, phi, data, noise_covariance, phi_covariance, field_covariance, mask, beam,
+                               n=n)
+    grad_f = gradf_logpdf(field, phi, data, field_covariance, noise_covariance, mask, beam, n=n)
+    chain = mixing_jacobian_phi_component(mixed_field, phi, grad_f, mixing_d, n=n)
+    return (pinv(mixing_g) * phi.replace(scalar_matrix=grad_phi + chain)).scalar_matrix
+
+
 # ---------------------------------------------------------- Wiener filter
 def hessian_logpdf_preconditioner(field_covariance, beam, mask, noise_covariance):
     """wiener_filter.py:36-43."""

@@ -10,7 +10,9 @@ this script:
 * outputs (lensed / adjoint-lensed fields, gradients) are stored as a seeded
   subsample of 8192 entries plus the row/column indices, so the fixtures stay
   small while still pinning every output;
-* logpdf scalars are stored exactly.
+* logpdf scalars are stored exactly;
+* ``mix.npz`` holds the mixing diagonals D (T, EE, BB) and G with the
+  subsampled mixed phi gradients (T-only and QU-only sets).
 
 Run once in a container that has the reference checked out::
 
@@ -70,6 +72,10 @@ def main(src):
                         b_ee=L("b_ee_P.npz"), b_bb=L("b_bb_P.npz"),
                         gradf_e=sub("gradf_e_P.npz"), gradf_b=sub("gradf_b_P.npz"), grad_phi=sub("grad_phi_t_P.npz"),
                         logpdf=float(open(os.path.join(src, "logpdf_P.txt")).read()))
+    # mixed parametrisation: mixing diagonals D, G in full, mixed phi gradients subsampled
+    np.savez_compressed(os.path.join(HERE, "mix.npz"), idx=idx, **meta,
+                        d_t=L("d_I.npz"), g=L("g_I.npz"), d_ee=L("d_ee_P.npz"), d_bb=L("d_bb_P.npz"),
+                        mixed_grad_phi_I=sub("mixed_grad_phi_I.npz"), mixed_grad_phi_P=sub("mixed_grad_phi_P.npz"))
     for f in sorted(os.listdir(HERE)):
         if f.endswith(".npz"):
             print(f, os.path.getsize(os.path.join(HERE, f)))
