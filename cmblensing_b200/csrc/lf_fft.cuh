@@ -234,6 +234,137 @@ __device__ __forceinline__ void fft_tiles(c2<T>* buf, const c2<T>* tw, int tid, 
   }
 }
 
+// ------------------------------------------------ register-level passes
+// The pieces of one Stockham pass over the LINES lines of a single tile, for
+// callers that keep a pass's outputs in registers: ``sp_read`` gathers the R
+// inputs of each of the thread's butterflies from ``src(m, line)`` (shared
+// memory or global), twiddles and transforms them; ``sp_apply`` /
+// ``sp_emit`` visit the outputs at their natural positions m; ``sp_write``
+// stores them to the tile.  Butterfly b of a thread is (line, j) =
+// (idx % LINES, idx / LINES) with idx = tid + b * NT, as in stockham_pass.
+template <int L, int R, int LINES, int NT> struct SpGeom {
+  static constexpr int NB = L / R;
+  static constexpr int TOT = NB * LINES;
+  static constexpr int PER = (TOT + NT - 1) / NT;
+};
+
+template <typename T, int L, int R, int NS, int LINES, int NT, bool INV, int NTAB, class Src>
+__device__ __forceinline__ void sp_read(c2<T> (&v)[SpGeom<L, R, LINES, NT>::PER][R], Src src,
+                                        const c2<T>* tw, int tid) {
+  using G = SpGeom<L, R, LINES, NT>;
+  constexpr int TWS = NTAB / (NS * R);
+  static_assert(NTAB % (NS * R) == 0, "twiddle table too small");
+#pragma unroll
+  for (int b = 0; b < G::PER; ++b) {
+    const int idx = tid + b * NT;
+    if (G::TOT % NT == 0 || idx < G::TOT) {
+      const int line = idx % LINES, j = idx / LINES;
+#pragma unroll
+      for (int r = 0; r < R; ++r) v[b][r] = src(j + r * G::NB, line);
+      if constexpr (NS > 1) {
+        const int k = j % NS;
+#pragma unroll
+        for (int r = 1; r < R; ++r) v[b][r] = twmul<T, INV>(v[b][r], tw[r * k * TWS]);
+      }
+      dft<R, T, INV>(v[b]);
+    }
+  }
+}
+
+// f(m, line, x) -> x' for every output of the thread's butterflies (in place).
+template <typename T, int L, int R, int NS, int LINES, int NT, class F>
+__device__ __forceinline__ void sp_apply(c2<T> (&v)[SpGeom<L, R, LINES, NT>::PER][R], F f, int tid) {
+  using G = SpGeom<L, R, LINES, NT>;
+#pragma unroll
+  for (int b = 0; b < G::PER; ++b) {
+    const int idx = tid + b * NT;
+    if (G::TOT % NT == 0 || idx < G::TOT) {
+      const int line = idx % LINES, j = idx / LINES;
+      const int base = (j / NS) * NS * R + j % NS;
+#pragma unroll
+      for (int r = 0; r < R; ++r) v[b][r] = f(base + r * NS, line, v[b][r]);
+    }
+  }
+}
+
+template <typename T, int L, int R, int NS, int LINES, int NT, class Dst>
+__device__ __forceinline__ void sp_emit(c2<T> (&v)[SpGeom<L, R, LINES, NT>::PER][R], Dst dst, int tid) {
+  sp_apply<T, L, R, NS, LINES, NT>(v, [=](int m, int line, c2<T> x) { dst(m, line, x); return x; }, tid);
+}
+
+template <typename T, int L, int R, int NS, int LINES, int NT>
+__device__ __forceinline__ void sp_write(c2<T>* buf, c2<T> (&v)[SpGeom<L, R, LINES, NT>::PER][R], int tid) {
+  sp_emit<T, L, R, NS, LINES, NT>(v, [=](int m, int line, c2<T> x) { buf[sw<T, LINES>(m, line)] = x; }, tid);
+}
+
+// src -> FFT -> mul -> IFFT -> dst for the LINES lines of one tile, with the
+// forward plan's last pass and the inverse plan's first pass fused in
+// registers.  The inverse runs the forward radices in reverse order, so both
+// fused passes have the same radix R and the same butterfly positions: the
+// forward pass leaves x[j + r L/R] in a thread's registers, which is exactly
+// the input set of the inverse pass's butterfly j.  The first pass reads
+// ``src(m, line)`` directly and the last pass hands its outputs to
+// ``dst(m, line, x)``, so shared memory sees 2 * (passes - 1) sweeps instead
+// of 2 * (2 passes + 1).  ``mul(m, line, x)`` gets the spectrum at frequency m.
+// Plans: 32 = 8x4, 64 = 8x8, 128 = 8x16, 256 = 16x16, 512 = 8x8x8, 1024 = 16x8x8.
+template <typename T, int L, int LINES, int NT, int NTAB, class Src, class Mul, class Dst>
+__device__ __forceinline__ void fft_mul_ifft(c2<T>* buf, const c2<T>* tw, int tid, Src src, Mul mul,
+                                             Dst dst) {
+  auto smem = [=](int m, int line) { return buf[sw<T, LINES>(m, line)]; };
+  constexpr int R1 = (L == 32 || L == 64 || L == 128 || L == 512) ? 8 : 16;
+  constexpr int R2 = (L == 32) ? 4 : (L == 64 || L == 512 || L == 1024) ? 8 : 16;
+  constexpr int R3 = (L == 512 || L == 1024) ? 8 : 1;
+  static_assert(L == 32 || L == 64 || L == 128 || L == 256 || L == 512 || L == 1024, "unsupported length");
+  if constexpr (R3 == 1) {
+    static_assert(R1 * R2 == L, "plan");
+    c2<T> a[SpGeom<L, R1, LINES, NT>::PER][R1];
+    c2<T> b[SpGeom<L, R2, LINES, NT>::PER][R2];
+    sp_read<T, L, R1, 1, LINES, NT, false, NTAB>(a, src, tw, tid);
+    sp_write<T, L, R1, 1, LINES, NT>(buf, a, tid);
+    __syncthreads();
+    sp_read<T, L, R2, R1, LINES, NT, false, NTAB>(b, smem, tw, tid);
+    sp_apply<T, L, R2, R1, LINES, NT>(b, mul, tid);
+#pragma unroll
+    for (int i = 0; i < SpGeom<L, R2, LINES, NT>::PER; ++i) {
+      if (SpGeom<L, R2, LINES, NT>::TOT % NT == 0 || tid + i * NT < SpGeom<L, R2, LINES, NT>::TOT)
+        dft<R2, T, true>(b[i]);
+    }
+    __syncthreads();
+    sp_write<T, L, R2, 1, LINES, NT>(buf, b, tid);
+    __syncthreads();
+    sp_read<T, L, R1, R2, LINES, NT, true, NTAB>(a, smem, tw, tid);
+    sp_emit<T, L, R1, R2, LINES, NT>(a, dst, tid);
+  } else {
+    static_assert(R1 * R2 * R3 == L, "plan");
+    c2<T> a[SpGeom<L, R1, LINES, NT>::PER][R1];
+    c2<T> b[SpGeom<L, R2, LINES, NT>::PER][R2];
+    c2<T> c[SpGeom<L, R3, LINES, NT>::PER][R3];
+    sp_read<T, L, R1, 1, LINES, NT, false, NTAB>(a, src, tw, tid);
+    sp_write<T, L, R1, 1, LINES, NT>(buf, a, tid);
+    __syncthreads();
+    sp_read<T, L, R2, R1, LINES, NT, false, NTAB>(b, smem, tw, tid);
+    __syncthreads();
+    sp_write<T, L, R2, R1, LINES, NT>(buf, b, tid);
+    __syncthreads();
+    sp_read<T, L, R3, R1 * R2, LINES, NT, false, NTAB>(c, smem, tw, tid);
+    sp_apply<T, L, R3, R1 * R2, LINES, NT>(c, mul, tid);
+#pragma unroll
+    for (int i = 0; i < SpGeom<L, R3, LINES, NT>::PER; ++i) {
+      if (SpGeom<L, R3, LINES, NT>::TOT % NT == 0 || tid + i * NT < SpGeom<L, R3, LINES, NT>::TOT)
+        dft<R3, T, true>(c[i]);
+    }
+    __syncthreads();
+    sp_write<T, L, R3, 1, LINES, NT>(buf, c, tid);
+    __syncthreads();
+    sp_read<T, L, R2, R3, LINES, NT, true, NTAB>(b, smem, tw, tid);
+    __syncthreads();
+    sp_write<T, L, R2, R3, LINES, NT>(buf, b, tid);
+    __syncthreads();
+    sp_read<T, L, R1, R3 * R2, LINES, NT, true, NTAB>(a, smem, tw, tid);
+    sp_emit<T, L, R1, R3 * R2, LINES, NT>(a, dst, tid);
+  }
+}
+
 // ----------------------------------------------------- real-FFT packing
 // Rows of N real samples are held as H = N/2 complex values z[m] = x[2m] + i x[2m+1].
 // The packed half spectrum of a row keeps X[k] for 1 <= k < H in slot k and

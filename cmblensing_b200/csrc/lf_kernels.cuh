@@ -120,22 +120,22 @@ __global__ void __launch_bounds__(NT, MINB) k_col(StageArgs a) {
   const int tid = threadIdx.x;
   const int c0 = blockIdx.x * LINES;
   const long plane = blockIdx.y;
+  static_assert(H % LINES == 0, "column tiles must cover the packed spectrum");
   load_twiddles<T, N, NT>(tw, a.twN, tid);
-  const c2<T>* in = reinterpret_cast<const c2<T>*>(a.s) + plane * (long)N * H;
-  c2<T>* out = reinterpret_cast<c2<T>*>(a.gx) + plane * (long)N * H;
-  load_cols<T, N, LINES, NT>(buf, in, H, c0, H, tid);
-  __syncthreads();
-  fft_tiles<T, N, LINES, 1, NT, false, N>(buf, tw, tid);
-  // i KX / N^2, folded into the first inverse pass; zero on KX's Nyquist row of
-  // the packed DC/Nyquist line (column 0)
+  const c2<T>* in = reinterpret_cast<const c2<T>*>(a.s) + plane * (long)N * H + c0;
+  c2<T>* out = reinterpret_cast<c2<T>*>(a.gx) + plane * (long)N * H + c0;
+  // i KX / N^2 between the transforms; zero on KX's Nyquist row of the packed
+  // DC/Nyquist line (column 0)
   const T scale = T(a.kbase / (double(N) * double(N)));
-  auto kx_mul = [=](int, int m, int line, c2<T> v) {
+  auto kx_mul = [=](int m, int line, c2<T> v) {
     const int kx = (m < N / 2) ? m : m - N;
     const T f = (c0 + line == 0 && m == N / 2) ? T(0) : scale * T(kx);
     return mk<T>(-f * v.y, f * v.x);
   };
-  fft_tiles<T, N, LINES, 1, NT, true, N>(buf, tw, tid, kx_mul);
-  store_cols<T, N, LINES, NT>(out, H, c0, H, buf, tid);
+  // rows of LINES consecutive columns: each warp's accesses cover whole 128-byte lines
+  auto src = [=](int m, int line) { return in[m * H + line]; };
+  auto dst = [=](int m, int line, c2<T> x) { out[m * H + line] = x; };
+  fft_mul_ifft<T, N, LINES, NT, N>(buf, tw, tid, src, kx_mul, dst);
 }
 
 // ========================================================= row pass
