@@ -57,18 +57,26 @@ int cuda_status(cudaError_t e) {
 // Launch geometry per (precision, N).
 template <typename T> struct Geo;
 // FP32 stage kernels: enough warps per SM to keep ~50 KB of loads in flight;
-// minb() caps registers at 64 per thread so that many blocks fit.
+// minb() caps registers at 64 per thread so that many blocks fit.  The row
+// pass runs 4-row tiles in half-size blocks: four blocks per SM (32 warps)
+// whose load, transform and epilogue phases drift apart keep HBM busier than
+// two 8-row blocks (7.46 vs 7.76 ms per 64-map 512^2 QU step; 2-row tiles in
+// eight blocks per SM: 8.73 ms).
 template <> struct Geo<float> {
   static constexpr int LINES = 16;     // column-pass tile
-  static constexpr int ROW_LINES = 8;  // row-pass tile (all C components at once)
+  static constexpr int ROW_LINES = 4;  // row-pass tile (all C components at once)
   static constexpr int nt(int n) { return n <= 64 ? 128 : (n <= 256 ? 256 : (n <= 512 ? 512 : 1024)); }
   static constexpr int minb(int n) { return 65536 / (nt(n) * 64); }
+  static constexpr int row_nt(int n) { return nt(n) / 2; }
+  static constexpr int row_minb(int n) { return 65536 / (row_nt(n) * 64); }
 };
 template <> struct Geo<double> {
   static constexpr int LINES = 8;
   static constexpr int ROW_LINES = 4;
   static constexpr int nt(int n) { return n <= 64 ? 64 : (n <= 128 ? 128 : (n <= 512 ? 256 : 512)); }
   static constexpr int minb(int) { return 1; }
+  static constexpr int row_nt(int n) { return nt(n); }
+  static constexpr int row_minb(int) { return 1; }
 };
 
 // Opt in to > 48 KB of dynamic shared memory once per kernel and device.
@@ -113,6 +121,8 @@ cudaError_t run_lens_n(const StageArgs& base, int B, int nsteps, double t0, doub
   constexpr int RL = Geo<T>::ROW_LINES;
   constexpr int NT = Geo<T>::nt(N);
   constexpr int MB = Geo<T>::minb(N);
+  constexpr int RNT = Geo<T>::row_nt(N);
+  constexpr int RMB = Geo<T>::row_minb(N);
   constexpr int H = N / 2;
   const size_t smem_row = sizeof(c2<T>) * (N + 2 * C * RL * H);
   const size_t smem_col = sizeof(c2<T>) * (N + LINES * N);
@@ -127,7 +137,7 @@ cudaError_t run_lens_n(const StageArgs& base, int B, int nsteps, double t0, doub
   a.last = 0;
   a.t_cur = t0;
   a.t_next = t0;
-  e = launch_k<k_row<T, N, C, ADJ, true, RL, NT, false, MB>>(LF_KIND_ROW, grow, NT, smem_row, st, a);
+  e = launch_k<k_row<T, N, C, ADJ, true, RL, RNT, false, RMB>>(LF_KIND_ROW, grow, RNT, smem_row, st, a);
   if (e != cudaSuccess) return e;
   for (int i = 0; i < nsteps; ++i) {
     const double t = t0 + i * h;  // util.py:189
@@ -140,7 +150,7 @@ cudaError_t run_lens_n(const StageArgs& base, int B, int nsteps, double t0, doub
       a.last = (i == nsteps - 1 && s == 3);
       e = launch_k<k_col<T, N, LINES, NT, MB>>(LF_KIND_COL, gcol, NT, smem_col, st, a);
       if (e != cudaSuccess) return e;
-      e = launch_k<k_row<T, N, C, ADJ, false, RL, NT, false, MB>>(LF_KIND_ROW, grow, NT, smem_row, st, a);
+      e = launch_k<k_row<T, N, C, ADJ, false, RL, RNT, false, RMB>>(LF_KIND_ROW, grow, RNT, smem_row, st, a);
       if (e != cudaSuccess) return e;
     }
   }
@@ -298,6 +308,8 @@ cudaError_t run_vjp_n(const StageArgs& af0, const StageArgs& ad0, double* dacc, 
   constexpr int RL = Geo<T>::ROW_LINES;
   constexpr int NT = Geo<T>::nt(N);
   constexpr int MB = Geo<T>::minb(N);
+  constexpr int RNT = Geo<T>::row_nt(N);
+  constexpr int RMB = Geo<T>::row_minb(N);
   constexpr int H = N / 2;
   const size_t smem_row = sizeof(c2<T>) * (N + 2 * C * RL * H);
   const size_t smem_col = sizeof(c2<T>) * (N + LINES * N);
@@ -313,9 +325,9 @@ cudaError_t run_vjp_n(const StageArgs& af0, const StageArgs& ad0, double* dacc, 
   af.stage = ad.stage = 0;
   af.last = ad.last = 0;
   af.t_cur = af.t_next = ad.t_cur = ad.t_next = t0;
-  cudaError_t e = launch_k<k_row<T, N, C, false, true, RL, NT, false, MB>>(LF_KIND_ROW, grow, NT, smem_row, st, af);
+  cudaError_t e = launch_k<k_row<T, N, C, false, true, RL, RNT, false, RMB>>(LF_KIND_ROW, grow, RNT, smem_row, st, af);
   if (e != cudaSuccess) return e;
-  e = launch_k<k_row<T, N, C, true, true, RL, NT, true, MB>>(LF_KIND_ROW, grow, NT, smem_row, st, ad);
+  e = launch_k<k_row<T, N, C, true, true, RL, RNT, true, RMB>>(LF_KIND_ROW, grow, RNT, smem_row, st, ad);
   if (e != cudaSuccess) return e;
   for (int i = 0; i < nsteps; ++i) {
     const double t = t0 + i * h;
@@ -329,14 +341,14 @@ cudaError_t run_vjp_n(const StageArgs& af0, const StageArgs& ad0, double* dacc, 
       af.last = ad.last = last;
       e = launch_k<k_col<T, N, LINES, NT, MB>>(LF_KIND_COL, gcol, NT, smem_col, st, af);
       if (e != cudaSuccess) return e;
-      e = launch_k<k_row<T, N, C, false, false, RL, NT, true, MB>>(LF_KIND_ROW, grow, NT, smem_row, st, af);
+      e = launch_k<k_row<T, N, C, false, false, RL, RNT, true, RMB>>(LF_KIND_ROW, grow, RNT, smem_row, st, af);
       if (e != cudaSuccess) return e;
       e = launch<k_dphi_accum<T, C>>(dim3(gacc), 256, 0, st, (const T*)af.grad, (const T*)ad.dsave,
                                      (const T*)af.phi, dacc, B, P, tc[s], h / 6.0 * cw[s], (int)(i == 0 && s == 0));
       if (e != cudaSuccess) return e;
       e = launch_k<k_col<T, N, LINES, NT, MB>>(LF_KIND_COL, gcol, NT, smem_col, st, ad);
       if (e != cudaSuccess) return e;
-      e = launch_k<k_row<T, N, C, true, false, RL, NT, true, MB>>(LF_KIND_ROW, grow, NT, smem_row, st, ad);
+      e = launch_k<k_row<T, N, C, true, false, RL, RNT, true, RMB>>(LF_KIND_ROW, grow, RNT, smem_row, st, ad);
       if (e != cudaSuccess) return e;
     }
   }
