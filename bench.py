@@ -214,17 +214,20 @@ def aggregate_value(world, batch_per_rank, steps, ms):
 
 
 # ----------------------------------------------------------- algorithmic bytes
-def row_bytes_per_lens(C, n, P, in_bytes=4, out_bytes=4):
-    """Bytes the row kernels of one forward lens must move per map (float32 state, 5 phi planes).
+def row_bytes_per_lens(C, n, P, in_bytes=4, out_bytes=4, p_planes=2):
+    """Bytes the row kernels of one forward lens must move per map (float32 state).
 
-    init: read f, write y0 and S.  Stage 1: read Gx, S, y0, phi(5); write acc, S.
-    Stages 2-3: also read acc.  Stage 4: read Gx, S, y0, acc, phi; write y0 and S
-    (the last stage writes the output instead and no S).
+    init: read f, write y0 and S.  Stage 1: read Gx, S, y0, the phi planes;
+    write acc, S.  Stages 2-3: also read acc.  Stage 4: read Gx, S, y0, acc,
+    phi planes; write y0 and S (the last stage writes the output instead and
+    no S).  ``p_planes`` = 2 when p is read at the stage time, 5 when it is
+    formed from the derivative planes.
     """
+    ph = 4 * p_planes
     init = (in_bytes + 8) * C
-    s1 = 20 * C + 20
-    s23 = 24 * C + 20
-    s4 = 24 * C + 20
+    s1 = 20 * C + ph
+    s23 = 24 * C + ph
+    s4 = 24 * C + ph
     last_adj = -8 * C + out_bytes * C  # last stage: no y0/S writes, one output write
     total = init + n * (s1 + 2 * s23 + s4) + last_adj
     return total * P
@@ -233,6 +236,11 @@ def row_bytes_per_lens(C, n, P, in_bytes=4, out_bytes=4):
 def col_bytes_per_lens(C, n, P):
     """Column kernels: read and write one row-spectral array (N x N/2 complex64 = 4P bytes) per plane."""
     return 4 * n * 8 * C * P
+
+
+def p_plane_bytes_per_lens(n, P):
+    """k_p_planes: read the five derivative planes, write p_x, p_y at the 2n+1 stage times."""
+    return (20 + 8 * (2 * n + 1)) * P
 
 
 def survey_bytes_per_map(C, n, P):
@@ -387,7 +395,7 @@ def main():
     phi_dev = torch.as_tensor(phi_host, device=dev)
     out_dev = torch.empty_like(f_dev)
     planes = torch.empty((B, 5, N, N), dtype=torch.float32, device=dev)
-    ws = torch.empty(plan.workspace_bytes(B, False), dtype=torch.uint8, device=dev)
+    ws = torch.empty(plan.workspace_bytes(B, False, n), dtype=torch.uint8, device=dev)
     phi_ws = torch.empty(plan.phi_workspace_bytes(B), dtype=torch.uint8, device=dev)
 
     def step():
@@ -423,6 +431,7 @@ def main():
     row_ms, row_n = plan.profile_read(nat.LF_KIND_ROW)
     col_ms, col_n = plan.profile_read(nat.LF_KIND_COL)
     phi_ms, phi_n = plan.profile_read(nat.LF_KIND_PHI)
+    pp_ms, pp_n = plan.profile_read(nat.LF_KIND_PP)
     ms = max_over_ranks(ms, dist, dev)
     value = aggregate_value(world, B, a.steps, ms)
 
@@ -443,6 +452,10 @@ def main():
     avg_s = (k_ms / max(k_n, 1)) / 1000.0
     achieved = k_b / avg_s / 1e9 if avg_s > 0 else 0.0
     step_gbs = survey_bytes_per_map(C, n, P) * (value / world) / 1e9
+    # the bytes this engine's path moves per map: row + column passes, phi
+    # precompute and the stage-time p planes
+    path_b = row_bytes_per_lens(C, n, P) + col_bytes_per_lens(C, n, P) + 140 * P + p_plane_bytes_per_lens(n, P)
+    path_gbs = path_b * (value / world) / 1e9
 
     result = {"metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": a.steps,
               "warmup": a.warmup, "ms_per_step": ms / a.steps, "higher_is_better": True, "scaling": "weak",
@@ -453,9 +466,11 @@ def main():
                            "peak_source": peak_src,
                            "bytes_per_launch": k_b, "avg_launch_ms": avg_s * 1000.0,
                            "step_model_gbs": step_gbs, "step_model_frac": step_gbs / hbm_peak,
-                           "step_model": "(4n(36C+20)+8C+140) N^2 bytes per map"},
-              "kernel_ms_per_step": {"row": row_ms / a.steps, "col": col_ms / a.steps, "phi": phi_ms / a.steps},
-              "gpu_launches": (row_n + col_n + phi_n) // a.steps * a.steps,
+                           "step_model": "(4n(36C+20)+8C+140) N^2 bytes per map",
+                           "step_path_bytes_per_map": path_b, "step_path_frac": path_gbs / hbm_peak},
+              "kernel_ms_per_step": {"row": row_ms / a.steps, "col": col_ms / a.steps, "phi": phi_ms / a.steps,
+                                     "p_planes": pp_ms / a.steps},
+              "gpu_launches": (row_n + col_n + phi_n + pp_n) // a.steps * a.steps,
               "clocks": clk}
 
     # ------------------------------------------------------------ e2e leg

@@ -36,6 +36,7 @@ SIGNATURES = {
     "lf_plan_create": (_i, [ctypes.POINTER(_vp), _i, _i, ctypes.c_double, _i]),
     "lf_plan_destroy": (_i, [_vp]),
     "lf_workspace_bytes": (_sz, [_vp, _i, _i]),
+    "lf_workspace_bytes_n": (_sz, [_vp, _i, _i, _i]),
     "lf_phi_planes_bytes": (_sz, [_vp, _i]),
     "lf_phi_workspace_bytes": (_sz, [_vp, _i]),
     "lf_phi_precompute": (_i, [_vp, _vp, _i, _i, _vp, _vp, _vp, _sz, _vp]),
@@ -58,6 +59,7 @@ LF_NOALLOC_SCRATCH_BYTES = 24 * 1024 * 1024
 LF_KIND_ROW = 0
 LF_KIND_COL = 1
 LF_KIND_PHI = 2
+LF_KIND_PP = 3
 
 
 class NativeLibraryError(RuntimeError):

@@ -115,8 +115,8 @@ cudaError_t launch(dim3 grid, int nt, size_t smem, cudaStream_t st, Args... args
   return launch_k<Kernel>(LF_KIND_PHI, grid, nt, smem, st, args...);
 }
 
-template <typename T, int N, int C, bool ADJ>
-cudaError_t run_lens_n(const StageArgs& base, int B, int nsteps, double t0, double t1, cudaStream_t st) {
+template <typename T, int N, int C, bool ADJ, bool PP>
+cudaError_t run_lens_pp(const StageArgs& base, int B, int nsteps, double t0, double t1, cudaStream_t st) {
   constexpr int LINES = Geo<T>::LINES;
   constexpr int RL = Geo<T>::ROW_LINES;
   constexpr int NT = Geo<T>::nt(N);
@@ -132,29 +132,52 @@ cudaError_t run_lens_n(const StageArgs& base, int B, int nsteps, double t0, doub
   cudaError_t e;
   const double h = (t1 - t0) / nsteps;  // util.py:185
   const double hh = h / 2.0;
+  if constexpr (PP) {
+    // p at the stage times t0 + k hh, k = 0..2n
+    const long P = (long)N * N;
+    a.pp_k = 2 * nsteps + 1;
+    const int gx = (int)std::min<long>((P / 2 + 255) / 256, 1024);
+    e = launch_k<k_p_planes<T>>(LF_KIND_PP, dim3(gx, B), 256, 0, st, reinterpret_cast<const T*>(a.phi),
+                                reinterpret_cast<T*>(const_cast<void*>(a.pp)), P, a.pp_k, t0, hh);
+    if (e != cudaSuccess) return e;
+  }
   a.h = h;
   a.stage = 0;
   a.last = 0;
   a.t_cur = t0;
   a.t_next = t0;
-  e = launch_k<k_row<T, N, C, ADJ, true, RL, RNT, false, RMB>>(LF_KIND_ROW, grow, RNT, smem_row, st, a);
+  a.pp_idx = 0;
+  e = launch_k<k_row<T, N, C, ADJ, true, RL, RNT, false, RMB, PP>>(LF_KIND_ROW, grow, RNT, smem_row, st, a);
   if (e != cudaSuccess) return e;
   for (int i = 0; i < nsteps; ++i) {
     const double t = t0 + i * h;  // util.py:189
     const double tc[4] = {t, t + hh, t + hh, t + h};
     const double tn[4] = {t + hh, t + hh, t + h, t0 + (i + 1) * h};
+    // the same times as indices k of t0 + k hh
+    const int kc[4] = {2 * i, 2 * i + 1, 2 * i + 1, 2 * i + 2};
+    const int kn[4] = {2 * i + 1, 2 * i + 1, 2 * i + 2, 2 * i + 2};
     for (int s = 0; s < 4; ++s) {
       a.stage = s + 1;
       a.t_cur = tc[s];
       a.t_next = tn[s];
+      a.pp_idx = ADJ ? kn[s] : kc[s];
       a.last = (i == nsteps - 1 && s == 3);
       e = launch_k<k_col<T, N, LINES, NT, MB>>(LF_KIND_COL, gcol, NT, smem_col, st, a);
       if (e != cudaSuccess) return e;
-      e = launch_k<k_row<T, N, C, ADJ, false, RL, RNT, false, RMB>>(LF_KIND_ROW, grow, RNT, smem_row, st, a);
+      e = launch_k<k_row<T, N, C, ADJ, false, RL, RNT, false, RMB, PP>>(LF_KIND_ROW, grow, RNT, smem_row, st, a);
       if (e != cudaSuccess) return e;
     }
   }
   return cudaSuccess;
+}
+
+// The p-plane path (a.pp set) is built for float32 plans only.
+template <typename T, int N, int C, bool ADJ>
+cudaError_t run_lens_n(const StageArgs& a, int B, int nsteps, double t0, double t1, cudaStream_t st) {
+  if constexpr (std::is_same<T, float>::value) {
+    if (a.pp) return run_lens_pp<T, N, C, ADJ, true>(a, B, nsteps, t0, t1, st);
+  }
+  return run_lens_pp<T, N, C, ADJ, false>(a, B, nsteps, t0, t1, st);
 }
 
 template <typename T, int N>
@@ -452,6 +475,17 @@ size_t lf_workspace_bytes(lf_plan_t p, int batch, int adjoint) {
   return el * (size_t)p->N * p->N * (size_t)batch * p->C * (adjoint ? 5 : 4);
 }
 
+// p-plane region: 2 (2n+1) planes per map, float32 plans only
+static size_t pp_bytes(lf_plan_t p, int batch, int nsteps) {
+  if (p->prec != LF_F32 || nsteps <= 0) return 0;
+  return 4 * (size_t)p->N * p->N * (size_t)batch * 2 * (2 * (size_t)nsteps + 1);
+}
+
+size_t lf_workspace_bytes_n(lf_plan_t p, int batch, int adjoint, int nsteps) {
+  if (!p || batch < 0 || nsteps < 0) return 0;
+  return lf_workspace_bytes(p, batch, adjoint) + pp_bytes(p, batch, nsteps);
+}
+
 size_t lf_phi_planes_bytes(lf_plan_t p, int batch) {
   if (!p || batch < 0) return 0;
   const size_t el = p->prec == LF_F64 ? 8 : 4;
@@ -533,6 +567,10 @@ int lf_lense_flow(lf_plan_t p, const void* f_in, int in_dtype, void* f_out, int 
   a.s = w + 2 * plane_bytes;
   a.gx = w + 3 * plane_bytes;
   a.v = adj ? (void*)(w + 4 * plane_bytes) : nullptr;
+  // room for the p planes: read p at the stage times instead of forming it
+  const size_t base_bytes = lf_workspace_bytes(p, batch, adj);
+  const size_t ppb = pp_bytes(p, batch, nsteps);
+  if (ppb && ws_bytes >= base_bytes + ppb) a.pp = w + base_bytes;
   a.twN = p->tw;
   a.kbase = 2.0 * M_PI / ((double)p->N * p->pix_width);
   a.nplanes = batch * p->C;

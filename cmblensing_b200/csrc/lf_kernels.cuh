@@ -48,6 +48,11 @@ struct StageArgs {
   // reverse-mode (VJP) extras
   void* grad;       // standard pass with SAVE: d_x y_s, d_y y_s, [B*C][2][N][N] T
   void* dsave;      // adjoint pass with SAVE: next stage input, [B*C][N][N] T
+  // p = M(t)^-1 grad(phi) at the 2n+1 stage times t0 + k h/2 (row pass with PP):
+  // [B][pp_k][2][N][N] T; this stage reads time index pp_idx
+  const void* pp;
+  int pp_k;
+  int pp_idx;
 };
 
 // p = M(t)^-1 grad(phi) with M = I + t grad grad phi (lense_flow.py:373-381, :398-415)
@@ -152,7 +157,10 @@ __global__ void __launch_bounds__(NT, MINB) k_col(StageArgs a) {
 // STAGE0: initialisation (copy the input field, transform the first stage
 // input), no rate.  SAVE (reverse mode): the standard pass also stores
 // d_x y_s and d_y y_s; the adjoint pass stores its next stage input.
-template <typename T, int N, int C, bool ADJ, bool STAGE0, int LINES, int NT, bool SAVE = false, int MINB = 1>
+// PP: p at the stage time is read from the precomputed p planes (two loads per
+// pixel) instead of being formed from the five derivative planes.
+template <typename T, int N, int C, bool ADJ, bool STAGE0, int LINES, int NT, bool SAVE = false, int MINB = 1,
+          bool PP = false>
 __global__ void __launch_bounds__(NT, MINB) k_row(StageArgs a) {
   constexpr int H = N / 2;
   constexpr long P = (long)N * N;
@@ -222,23 +230,35 @@ __global__ void __launch_bounds__(NT, MINB) k_row(StageArgs a) {
   for (int idx = tid; idx < E2 * LINES; idx += NT) {
     const int row = idx / E2, m0 = 2 * (idx % E2);
     const long e0 = (long)row * H + m0;  // packed-element index within the tile
-    c2<T> fx[2], fy[2], fxx[2], fxy[2], fyy[2];
     const bool need_phi = STAGE0 ? ADJ : (!ADJ || live);
-    if (need_phi) {
-      ld2<T>(reinterpret_cast<const c2<T>*>(phi) + e0, fx);
-      ld2<T>(reinterpret_cast<const c2<T>*>(phi + P) + e0, fy);
-      ld2<T>(reinterpret_cast<const c2<T>*>(phi + 2 * P) + e0, fxx);
-      ld2<T>(reinterpret_cast<const c2<T>*>(phi + 3 * P) + e0, fxy);
-      ld2<T>(reinterpret_cast<const c2<T>*>(phi + 4 * P) + e0, fyy);
-    }
     // p at the rate time (standard) and at the next stage time (adjoint)
     T prx[2][2], pry[2][2];
     if (need_phi) {
-      const T tp = ADJ ? tnext : tcur;
+      if constexpr (PP) {
+        const T* pp = reinterpret_cast<const T*>(a.pp) + (map * a.pp_k + a.pp_idx) * 2 * P + (long)r0 * N;
+        c2<T> px[2], py[2];
+        ld2<T>(reinterpret_cast<const c2<T>*>(pp) + e0, px);
+        ld2<T>(reinterpret_cast<const c2<T>*>(pp + P) + e0, py);
 #pragma unroll
-      for (int q = 0; q < 2; ++q) {
-        p_vector<T>(fx[q].x, fy[q].x, fxx[q].x, fxy[q].x, fyy[q].x, tp, prx[q][0], pry[q][0]);
-        p_vector<T>(fx[q].y, fy[q].y, fxx[q].y, fxy[q].y, fyy[q].y, tp, prx[q][1], pry[q][1]);
+        for (int q = 0; q < 2; ++q) {
+          prx[q][0] = px[q].x;
+          prx[q][1] = px[q].y;
+          pry[q][0] = py[q].x;
+          pry[q][1] = py[q].y;
+        }
+      } else {
+        c2<T> fx[2], fy[2], fxx[2], fxy[2], fyy[2];
+        ld2<T>(reinterpret_cast<const c2<T>*>(phi) + e0, fx);
+        ld2<T>(reinterpret_cast<const c2<T>*>(phi + P) + e0, fy);
+        ld2<T>(reinterpret_cast<const c2<T>*>(phi + 2 * P) + e0, fxx);
+        ld2<T>(reinterpret_cast<const c2<T>*>(phi + 3 * P) + e0, fxy);
+        ld2<T>(reinterpret_cast<const c2<T>*>(phi + 4 * P) + e0, fyy);
+        const T tp = ADJ ? tnext : tcur;
+#pragma unroll
+        for (int q = 0; q < 2; ++q) {
+          p_vector<T>(fx[q].x, fy[q].x, fxx[q].x, fxy[q].x, fyy[q].x, tp, prx[q][0], pry[q][0]);
+          p_vector<T>(fx[q].y, fy[q].y, fxx[q].y, fxy[q].y, fyy[q].y, tp, prx[q][1], pry[q][1]);
+        }
       }
     }
 #pragma unroll
@@ -325,6 +345,32 @@ __global__ void __launch_bounds__(NT, MINB) k_row(StageArgs a) {
   for (int c = 0; c < C; ++c) {
     store_rows<T, c2<T>, H, LINES, NT>(spec(a.s, c), H, buf + c * TILE, tid);
     if constexpr (ADJ) store_rows<T, c2<T>, H, LINES, NT>(spec(a.v, c), H, buf + (C + c) * TILE, tid);
+  }
+}
+
+// ====================================================== p planes
+// p = M(t)^-1 grad(phi), M = I + t grad grad phi (lense_flow.py:373-381,
+// :398-415), at the K = 2n+1 stage times t_k = t0 + k hh of an RK4
+// integration, from the five derivative planes; float64 arithmetic, stored in
+// T.  grid: x covers P/2 pixel pairs, y = map.
+template <typename T>
+__global__ void __launch_bounds__(256) k_p_planes(const T* __restrict__ planes, T* __restrict__ pp, long P, int K,
+                                                  double t0, double hh) {
+  const long map = blockIdx.y;
+  const T* ph = planes + map * 5 * P;
+  T* out = pp + map * (long)K * 2 * P;
+  for (long i = blockIdx.x * (long)blockDim.x + threadIdx.x; i < P / 2; i += (long)gridDim.x * blockDim.x) {
+    c2<T> f[5];
+#pragma unroll
+    for (int j = 0; j < 5; ++j) f[j] = reinterpret_cast<const c2<T>*>(ph + j * P)[i];
+    for (int k = 0; k < K; ++k) {
+      const double t = t0 + k * hh;
+      double ox[2], oy[2];
+      p_vector<double>(f[0].x, f[1].x, f[2].x, f[3].x, f[4].x, t, ox[0], oy[0]);
+      p_vector<double>(f[0].y, f[1].y, f[2].y, f[3].y, f[4].y, t, ox[1], oy[1]);
+      reinterpret_cast<c2<T>*>(out + (2 * k) * P)[i] = mk<T>(T(ox[0]), T(ox[1]));
+      reinterpret_cast<c2<T>*>(out + (2 * k + 1) * P)[i] = mk<T>(T(oy[0]), T(oy[1]));
+    }
   }
 }
 

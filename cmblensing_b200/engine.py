@@ -52,8 +52,11 @@ class Plan:
             pass
 
     # -------------------------------------------------------------- sizes
-    def workspace_bytes(self, batch, adjoint):
-        return int(self._lib.lf_workspace_bytes(self.handle, int(batch), int(bool(adjoint))))
+    def workspace_bytes(self, batch, adjoint, n=None):
+        """Lens workspace; with ``n`` RK4 steps, the size that also holds the stage-time p planes."""
+        if n is None:
+            return int(self._lib.lf_workspace_bytes(self.handle, int(batch), int(bool(adjoint))))
+        return int(self._lib.lf_workspace_bytes_n(self.handle, int(batch), int(bool(adjoint)), int(n)))
 
     def phi_planes_bytes(self, batch):
         return int(self._lib.lf_phi_planes_bytes(self.handle, int(batch)))
@@ -120,9 +123,11 @@ class Plan:
         odt = f.dtype if out_dtype is None else out_dtype
         if out is None:
             out = torch.empty((B, C, N, N), dtype=odt, device=self.device)
-        need = self.workspace_bytes(B, adjoint)
-        if workspace is None or workspace.numel() < need:
-            workspace = torch.empty(max(need, 16), dtype=torch.uint8, device=self.device)
+        # a caller's workspace of at least the minimum is used as given (the
+        # engine reads the p planes only when it also has room for them)
+        if workspace is None or workspace.numel() < self.workspace_bytes(B, adjoint):
+            workspace = torch.empty(max(self.workspace_bytes(B, adjoint, n), 16), dtype=torch.uint8,
+                                    device=self.device)
         code = lambda t: nat.LF_F64 if t == torch.float64 else nat.LF_F32
         with torch.cuda.device(self.device):
             nat.check(self._lib.lf_lense_flow(self.handle, _ptr(f), code(f.dtype), _ptr(out), code(out.dtype),
@@ -243,7 +248,7 @@ class HostPipeline:
         self.d_out = [torch.empty((cb, C, N, N), dtype=io_dtype, device=dev) for _ in range(2)]
         self.d_phi = [torch.empty((cb, N, N), dtype=torch.float64, device=dev) for _ in range(2)]
         self.planes = torch.empty((cb, 5, N, N), dtype=plan.dtype, device=dev)
-        self.ws = torch.empty(max(plan.workspace_bytes(cb, True), 16), dtype=torch.uint8, device=dev)
+        self.ws = torch.empty(16, dtype=torch.uint8, device=dev)  # sized for n at the first call
         self.phi_ws = torch.empty(max(plan.phi_workspace_bytes(cb), 16), dtype=torch.uint8, device=dev)
         self.min_det = torch.empty(max(self.chunks * cb, 1), dtype=torch.int32, device=dev)
         self.s_in = torch.cuda.Stream(dev)
@@ -260,6 +265,9 @@ class HostPipeline:
 
     def __call__(self, f_host, phi_host, out_host, n=10, direction=FORWARD_LENSE, adjoint=False, check_det=True):
         plan, lib = self.plan, self.plan._lib
+        need = plan.workspace_bytes(self.cb, True, n)
+        if self.ws.numel() < need:
+            self.ws = torch.empty(need, dtype=torch.uint8, device=plan.device)
         cur = torch.cuda.current_stream(plan.device)
         for st in (self.s_in, self.s_cmp, self.s_out):
             st.wait_stream(cur)

@@ -97,7 +97,7 @@ class _LensSlot:
         self.d_phi = torch.empty((cap, N, N), dtype=torch.float64, device=dev)
         self.d_out = torch.empty_like(self.d_f)
         self.planes = torch.empty((cap, 5, N, N), dtype=torch.float32, device=dev)
-        self.ws = torch.empty(max(self.plan.workspace_bytes(cap, True), 16), dtype=torch.uint8, device=dev)
+        self.ws = torch.empty(max(self.plan.workspace_bytes(cap, True, n), 16), dtype=torch.uint8, device=dev)
         self.phi_ws = torch.empty(max(self.plan.phi_workspace_bytes(cap), 16), dtype=torch.uint8, device=dev)
         self.md = torch.empty(cap, dtype=torch.int32, device=dev)
         self.stream = torch.cuda.Stream(dev)

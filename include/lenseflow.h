@@ -62,6 +62,13 @@ int lf_plan_destroy(lf_plan_t plan);
 
 /* Bytes of caller workspace needed by lf_lense_flow for ``batch`` maps. */
 size_t lf_workspace_bytes(lf_plan_t plan, int batch, int adjoint);
+/* Workspace with which lf_lense_flow of a float32 plan also precomputes
+ * p = M(t)^-1 grad(phi) at the 2 nsteps + 1 RK4 stage times (lense_flow.py:
+ * 373-381, :398-415; two planes per time and map) so that every row pass
+ * reads two planes per pixel instead of five.  lf_lense_flow takes that path
+ * whenever ws_bytes is at least this; with at least lf_workspace_bytes it
+ * forms p from the derivative planes in every stage. */
+size_t lf_workspace_bytes_n(lf_plan_t plan, int batch, int adjoint, int nsteps);
 /* Bytes of the derivative-plane buffer for ``batch`` maps. */
 size_t lf_phi_planes_bytes(lf_plan_t plan, int batch);
 /* Bytes of float64 scratch needed by lf_phi_precompute for ``batch`` maps. */
@@ -142,7 +149,7 @@ int lf_lense_flow_noalloc(int nside, int ncomp, double pix_width, const void* f_
  * lf_profile_read synchronises on the last event and returns the summed
  * duration and count of the recorded launches of one kind.  No counterpart
  * in the reference (its device work is XLA-generated). */
-enum lf_kernel_kind { LF_KIND_ROW = 0, LF_KIND_COL = 1, LF_KIND_PHI = 2 };
+enum lf_kernel_kind { LF_KIND_ROW = 0, LF_KIND_COL = 1, LF_KIND_PHI = 2, LF_KIND_PP = 3 };
 int lf_profile_enable(lf_plan_t plan, int enable);
 int lf_profile_reset(lf_plan_t plan);
 int lf_profile_read(lf_plan_t plan, int kind, double* total_ms, int* launches);

@@ -51,6 +51,7 @@ def test_plan_rejects_bad_arguments_before_touching_the_device(lib):
 
 def test_null_plan_calls_return_status(lib):
     assert lib.lf_workspace_bytes(None, 4, 0) == 0
+    assert lib.lf_workspace_bytes_n(None, 4, 0, 7) == 0
     assert lib.lf_lense_flow(None, None, 0, None, 0, None, 1, 7, 1, 0, None, 0, None) == nat.LF_ERR_BAD_ARG
     assert lib.lf_phi_precompute(None, None, 0, 1, None, None, None, 0, None) == nat.LF_ERR_BAD_ARG
     assert lib.lf_plan_destroy(None) == nat.LF_OK

@@ -56,6 +56,34 @@ def test_lens_matches_oracle(torch_cuda, N, theta, C, direction, adjoint):
         assert rel_l2(got[c], ref[c]) < TOL32, (c, rel_l2(got[c], ref[c]))
 
 
+@pytest.mark.parametrize("C,direction,adjoint", [(2, 1, False), (2, -1, False), (1, 1, True), (3, -1, True)])
+def test_p_plane_and_derivative_plane_paths(torch_cuda, C, direction, adjoint):
+    """A workspace of lf_workspace_bytes_n selects the stage-time p planes; one of lf_workspace_bytes the
+    five-plane path.  Both match the oracle and each other (the p planes are formed in float64)."""
+    import torch
+    from cmblensing_b200 import engine
+    N, theta, n = 128, 3.0, 7
+    f, phis = _inputs(N, theta, C, B=2, seed0=5)
+    pw = R.pix_width_of(theta)
+    plan = engine.get_plan(N, C, pw)
+    planes = plan.phi_planes(torch.as_tensor(phis, device="cuda"))
+    ft = torch.as_tensor(f, device="cuda", dtype=torch.float32)
+    small = plan.workspace_bytes(2, adjoint)
+    full = plan.workspace_bytes(2, adjoint, n)
+    assert full > small
+    outs = []
+    for nbytes in (small, full):
+        ws = torch.empty(nbytes, dtype=torch.uint8, device="cuda")
+        outs.append(plan.lense_flow(ft, planes, n=n, direction=direction, adjoint=adjoint,
+                                    workspace=ws).double().cpu().numpy())
+    for b in range(2):
+        ref = _oracle(f[b], phis[b], pw, n, direction, adjoint)
+        for out in outs:
+            for c in range(C):
+                assert rel_l2(out[b, c], ref[c]) < TOL32
+    assert rel_l2(outs[0], outs[1]) < 1e-6
+
+
 def test_lens_1024_T(torch_cuda):
     f, phis = _inputs(1024, 2.0, 1)
     pw = R.pix_width_of(2.0)
