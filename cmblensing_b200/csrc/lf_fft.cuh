@@ -1,16 +1,21 @@
 // Shared-memory FFT engine for the LenseFlow kernels (sm_100a).
 //
 // A thread block owns a *tile* of LINES independent 1-D transforms ("lines"),
-// each of length L, held in shared memory as complex values laid out
+// each of length L, held in shared memory as complex values.  Element
+// (m, line) -- m the position along the transform axis -- has the linear
+// index e = m * LINES + line and is stored at
 //
-//     element (m, line)  at  tile[m * LINES + (line ^ (m & (LINES - 1)))]
+//     tile[e ^ ((e / EPC) & (EPC - 1))],   EPC = 128 bytes / element size,
 //
-// m is the position along the transform axis.  The XOR swizzle makes both
-// access patterns used by the kernels bank-conflict free:
-//   * line-major  (consecutive threads = consecutive lines, same m): the
-//     Stockham passes and the real-FFT pre/post processing;
-//   * row-major   (consecutive threads = consecutive m, same line): the
-//     coalesced global loads/stores of row tiles and the pointwise epilogues.
+// i.e. every 128-byte chunk of the tile is permuted by an XOR with its chunk
+// number.  These warp access patterns then touch each bank at most twice
+// per 32 accesses (the minimum for 8-byte elements): the Stockham reads
+// (consecutive threads = consecutive lines, then consecutive m), the
+// Stockham writes at stride R in m, the row-major global loads and stores and
+// the pointwise epilogues (consecutive threads = consecutive m); the
+// descending H-k accesses of the real-FFT pre-pass reach three on some warps.
+// Permuting whole chunks rather than the lines of one m matters for tiles of
+// fewer than 16 lines, whose stride-R writes otherwise fall on LINES banks.
 //
 // The transforms are radix-R Stockham autosort passes (Govindaraju et al.,
 // "High performance discrete Fourier transforms on graphics processors",
@@ -133,16 +138,17 @@ template <int R, typename T, bool INV> __device__ __forceinline__ void dft(c2<T>
 }
 
 // ------------------------------------------------------------ tile layout
-// The XOR key changes every (128 bytes / (LINES x element size)) rows so
-// that 16 (8-byte elements) or 8 (16-byte elements) consecutive m of one
-// line land in distinct banks: m & 15 for 16 float2 lines, (m >> 1) & 7 for
-// 8 float2 lines, m & 7 for 8 double2 lines.
+// (0 <= line < LINES; the chunk number is written per case so that it costs
+// no more than a shift)
 template <typename T, int LINES> __device__ __forceinline__ int sw(int m, int line) {
-  constexpr int ROWS_PER_128B = (128 / int(sizeof(c2<T>))) / LINES;
-  if constexpr (ROWS_PER_128B >= 2) {
-    return m * LINES + (line ^ ((m / ROWS_PER_128B) & (LINES - 1)));
+  constexpr int EPC = 128 / int(sizeof(c2<T>));  // elements per 128-byte chunk
+  static_assert(LINES % EPC == 0 || EPC % LINES == 0, "LINES must divide or be a multiple of a chunk");
+  if constexpr (LINES == EPC) {
+    return m * LINES + (line ^ (m & (EPC - 1)));
+  } else if constexpr (LINES > EPC) {
+    return (m * LINES + line) ^ ((m * (LINES / EPC) + line / EPC) & (EPC - 1));
   } else {
-    return m * LINES + (line ^ (m & (LINES - 1)));
+    return (m * LINES + line) ^ ((m / (EPC / LINES)) & (EPC - 1));
   }
 }
 
