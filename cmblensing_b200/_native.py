@@ -37,6 +37,7 @@ SIGNATURES = {
     "lf_plan_destroy": (_i, [_vp]),
     "lf_workspace_bytes": (_sz, [_vp, _i, _i]),
     "lf_workspace_bytes_n": (_sz, [_vp, _i, _i, _i]),
+    "lf_wait_timeouts": (_i, [ctypes.POINTER(ctypes.c_int), _i]),
     "lf_phi_planes_bytes": (_sz, [_vp, _i]),
     "lf_phi_workspace_bytes": (_sz, [_vp, _i]),
     "lf_phi_precompute": (_i, [_vp, _vp, _i, _i, _vp, _vp, _vp, _sz, _vp]),

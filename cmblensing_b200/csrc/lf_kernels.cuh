@@ -348,6 +348,240 @@ __global__ void __launch_bounds__(NT, MINB) k_row(StageArgs a) {
   }
 }
 
+// ============================================ bulk copies and bounded waits
+// Set (never cleared by the kernels) when a block gave up waiting for its
+// bulk copies; the host reads it with lf_wait_timeouts().
+__device__ int g_lf_wait_timeouts;
+
+__device__ __forceinline__ uint32_t smem_addr(const void* p) {
+  return static_cast<uint32_t>(__cvta_generic_to_shared(p));
+}
+
+__device__ __forceinline__ void mbar_init(uint64_t* mbar, int count) {
+  asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(smem_addr(mbar)), "r"(count) : "memory");
+  // make the initialised barrier visible to the bulk-copy (async) proxy
+  asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+}
+
+__device__ __forceinline__ void mbar_expect_tx(uint64_t* mbar, uint32_t bytes) {
+  asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(smem_addr(mbar)), "r"(bytes)
+               : "memory");
+}
+
+// One contiguous global -> shared copy of ``bytes`` (16-byte aligned, multiple of 16).
+__device__ __forceinline__ void bulk_g2s(void* dst, const void* src, uint32_t bytes, uint64_t* mbar) {
+  asm volatile(
+      "cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];" ::"r"(
+          smem_addr(dst)),
+      "l"(src), "r"(bytes), "r"(smem_addr(mbar))
+      : "memory");
+}
+
+// Wait for phase ``parity`` of the barrier, giving up after ``tries`` polls;
+// each poll suspends for at most about 1 microsecond (the explicit time hint),
+// so a wait is bounded by roughly tries microseconds.
+__device__ __forceinline__ bool mbar_wait(uint64_t* mbar, uint32_t parity, int tries) {
+  const uint32_t addr = smem_addr(mbar);
+  for (int i = 0; i < tries; ++i) {
+    uint32_t done;
+    asm volatile(
+        "{\n .reg .pred p;\n mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2, %3;\n selp.u32 %0, 1, 0, p;\n}"
+        : "=r"(done)
+        : "r"(addr), "r"(parity), "r"(1000u)
+        : "memory");
+    if (done) return true;
+  }
+  return false;
+}
+
+constexpr int kWaitTries = 1 << 20;  // about one second
+
+// ============================================ row pass, component pairs
+// Standard RHS for two components (Q, U) with the p planes, N = 512, FP32.
+// The general row pass inverse-transforms four packed half spectra per row
+// (d_x and d_y of both components) and forward-transforms two, each as a
+// half-length complex FFT with a real-FFT pre/post pass in shared memory.
+// Here each component's two Hermitian derivative spectra are combined into
+// one full-length spectrum Z = DX + i DY, whose inverse FFT is dx + i dy;
+// after the RK4 update the two next stage inputs are combined into
+// w = y_0 + i y_1, whose forward FFT W gives both packed row spectra:
+// S_0[k] = (W[k] + conj W[N-k]) / 2, S_1[k] = (W[k] - conj W[N-k]) / 2i.
+// The Hermitian expansion and the split are local in k, so they happen in the
+// 16-byte global load and store phases, and the inverse transform's last
+// radix-8 pass, the pointwise update and the forward transform's first pass
+// run in registers: both passes see x[j + 64 r] of one row in one thread.
+// The update's operands (y0, acc, p_x, p_y of the tile's rows: contiguous
+// blocks) are fetched into shared memory by bulk copies issued at the start,
+// so their latency overlaps the loads and the first inverse passes.
+template <int LINES>
+constexpr size_t row_pair_smem_bytes(int n) {
+  return sizeof(float2) * (n + 2 * LINES * n) + sizeof(float) * 6 * LINES * n + 16;
+}
+
+template <int N, int LINES, int NT, int MINB>
+__global__ void __launch_bounds__(NT, MINB) k_row_pair(StageArgs a) {
+  using T = float;
+  constexpr int H = N / 2;
+  constexpr long P = (long)N * N;
+  constexpr int R = 8, NB = N / R;  // radix-8 passes: NB butterflies per row
+  static_assert(N == 512, "three radix-8 passes");
+  static_assert(NB * LINES == NT, "one (row, butterfly) per thread in the fused passes");
+  constexpr int TILE = LINES * N;
+  constexpr int RB = LINES * N;  // floats per staged row block
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  c2<T>* tw = reinterpret_cast<c2<T>*>(smem_raw);
+  c2<T>* buf = tw + N;                                 // tile c at buf + c * TILE
+  T* stg = reinterpret_cast<T*>(buf + 2 * TILE);       // y0_0, y0_1, acc_0, acc_1, p_x, p_y
+  uint64_t* mbar = reinterpret_cast<uint64_t*>(stg + 6 * RB);
+  const int tid = threadIdx.x;
+  const int r0 = blockIdx.x * LINES;
+  const long map = blockIdx.y;
+  const long prow0 = (long)r0 * N;
+  const bool with_acc = a.stage > 1;
+  if (tid == 0) {
+    mbar_init(mbar, 1);
+    mbar_expect_tx(mbar, uint32_t((with_acc ? 6 : 4) * RB * sizeof(T)));
+    const T* pp = reinterpret_cast<const T*>(a.pp) + (map * a.pp_k + a.pp_idx) * 2 * P + prow0;
+    for (int c = 0; c < 2; ++c) {
+      bulk_g2s(stg + c * RB, reinterpret_cast<const T*>(a.y0) + (map * 2 + c) * P + prow0, RB * sizeof(T), mbar);
+      if (with_acc)
+        bulk_g2s(stg + (2 + c) * RB, reinterpret_cast<const T*>(a.acc) + (map * 2 + c) * P + prow0, RB * sizeof(T),
+                 mbar);
+      bulk_g2s(stg + (4 + c) * RB, pp + c * P, RB * sizeof(T), mbar);
+    }
+  }
+  load_twiddles<T, N, NT>(tw, a.twN, tid);
+  const T ky_scale = T(a.kbase / double(N));
+  const long half_plane = N * (long)H;
+  auto spec = [&](void* base, int c) {
+    return reinterpret_cast<c2<T>*>(base) + (map * 2 + c) * half_plane + (long)r0 * H;
+  };
+
+  // ------------------------- load: Z_c = DX_c + i DY_c with DY = i KY S / N
+  // (slot 0 of a packed spectrum holds the real DC and Nyquist bins; the d_y
+  // spectrum has none: KY's DC and Nyquist terms vanish after irfft)
+#pragma unroll
+  for (int idx = tid; idx < 2 * LINES * (H / 2); idx += NT) {
+    const int t = idx % (H / 2);
+    const int rest = idx / (H / 2);
+    const int row = rest % LINES, c = rest / LINES;
+    c2<T> g[2], s[2];
+    ld2<T>(spec(a.gx, c) + row * H + 2 * t, g);
+    ld2<T>(spec(a.s, c) + row * H + 2 * t, s);
+    c2<T>* z = buf + c * TILE;
+#pragma unroll
+    for (int q = 0; q < 2; ++q) {
+      const int k = 2 * t + q;
+      if (k == 0) {
+        z[sw<T, LINES>(0, row)] = mk<T>(g[0].x, T(0));
+        z[sw<T, LINES>(H, row)] = mk<T>(g[0].y, T(0));
+      } else {
+        const T f = ky_scale * T(k);
+        const T dyx = -f * s[q].y, dyy = f * s[q].x;  // DY = i f S
+        z[sw<T, LINES>(k, row)] = mk<T>(g[q].x - dyy, g[q].y + dyx);       // DX + i DY
+        z[sw<T, LINES>(N - k, row)] = mk<T>(g[q].x + dyy, dyx - g[q].y);   // conj(DX) + i conj(DY)
+      }
+    }
+  }
+  __syncthreads();
+  stockham_pass<T, N, R, 1, LINES, 2, NT, true, N>(buf, tw, tid);
+  stockham_pass<T, N, R, R, LINES, 2, NT, true, N>(buf, tw, tid);
+
+  // ----------------- inverse pass 3 -> RK4 update -> forward pass 1, in registers
+  const int j = tid % NB, row = tid / NB;
+  c2<T> v[2][R];
+#pragma unroll
+  for (int c = 0; c < 2; ++c) {
+#pragma unroll
+    for (int r = 0; r < R; ++r) v[c][r] = buf[c * TILE + sw<T, LINES>(j + r * NB, row)];
+  }
+#pragma unroll
+  for (int r = 1; r < R; ++r) {
+    const c2<T> w = tw[r * j];  // W_N^(r j): NS = N / R
+#pragma unroll
+    for (int c = 0; c < 2; ++c) v[c][r] = twmul<T, true>(v[c][r], w);
+  }
+  dft<R, T, true>(v[0]);
+  dft<R, T, true>(v[1]);
+  // v[c][r] = dx + i dy of component c at pixel n = j + NB r of row r0 + row
+  if (!mbar_wait(mbar, 0, kWaitTries)) {
+    // the staged operands never arrived: record it, let the copies drain, leave
+    atomicExch(&g_lf_wait_timeouts, 1);
+    mbar_wait(mbar, 0, kWaitTries);
+    return;
+  }
+  const long prow = prow0 + (long)row * N;
+  const T* sy0 = stg + row * N;
+  const T* sacc = stg + 2 * RB + row * N;
+  const T* spx = stg + 4 * RB + row * N;
+  const T* spy = stg + 5 * RB + row * N;
+  const T hh = T(a.h);
+#pragma unroll
+  for (int r = 0; r < R; ++r) {
+    const int n = j + NB * r;
+    const T px = spx[n], py = spy[n];
+#pragma unroll
+    for (int c = 0; c < 2; ++c) {
+      const T k = px * v[c][r].x + py * v[c][r].y;
+      const T y0 = sy0[c * RB + n];
+      T* accg = reinterpret_cast<T*>(a.acc) + (map * 2 + c) * P + prow;
+      T yn;
+      if (a.stage == 1) {
+        yn = y0 + T(0.5) * hh * k;
+        accg[n] = k;
+      } else if (a.stage < 4) {
+        yn = y0 + (a.stage == 2 ? T(0.5) * hh : hh) * k;
+        accg[n] = sacc[c * RB + n] + T(2) * k;
+      } else {
+        yn = y0 + hh / T(6) * (sacc[c * RB + n] + k);
+        if (a.last) {
+          const long fo = (map * 2 + c) * P + prow + n;
+          if (a.out_f64) reinterpret_cast<double*>(a.f_out)[fo] = double(yn);
+          else reinterpret_cast<float*>(a.f_out)[fo] = yn;
+        } else {
+          reinterpret_cast<T*>(a.y0)[(map * 2 + c) * P + prow + n] = yn;
+        }
+      }
+      v[c][r].x = yn;
+    }
+  }
+  if (a.last) return;  // uniform across the block
+  c2<T> w[R];
+#pragma unroll
+  for (int r = 0; r < R; ++r) w[r] = mk<T>(v[0][r].x, v[1][r].x);
+  dft<R, T, false>(w);  // forward pass 1 (NS = 1): outputs at 8 j + r
+  __syncthreads();      // every thread has read its inverse-pass-3 inputs
+#pragma unroll
+  for (int r = 0; r < R; ++r) buf[sw<T, LINES>(R * j + r, row)] = w[r];
+  __syncthreads();
+  stockham_pass<T, N, R, R, LINES, 1, NT, false, N>(buf, tw, tid);
+  stockham_pass<T, N, R, R * R, LINES, 1, NT, false, N>(buf, tw, tid);
+
+  // ------------------------------ split W into the two packed row spectra
+#pragma unroll
+  for (int idx = tid; idx < LINES * (H / 2); idx += NT) {
+    const int t = idx % (H / 2), rw = idx / (H / 2);
+    c2<T> s0[2], s1[2];
+#pragma unroll
+    for (int q = 0; q < 2; ++q) {
+      const int k = 2 * t + q;
+      if (k == 0) {
+        const c2<T> w0 = buf[sw<T, LINES>(0, rw)], wh = buf[sw<T, LINES>(H, rw)];
+        s0[0] = mk<T>(w0.x, wh.x);
+        s1[0] = mk<T>(w0.y, wh.y);
+      } else {
+        const c2<T> A = buf[sw<T, LINES>(k, rw)];
+        const c2<T> B = cconj<T>(buf[sw<T, LINES>(N - k, rw)]);
+        s0[q] = cscale<T>(cadd<T>(A, B), T(0.5));
+        const c2<T> d = csub<T>(A, B);
+        s1[q] = mk<T>(T(0.5) * d.y, T(-0.5) * d.x);  // (A - B) / 2i
+      }
+    }
+    st2<T>(spec(a.s, 0) + rw * H + 2 * t, s0);
+    st2<T>(spec(a.s, 1) + rw * H + 2 * t, s1);
+  }
+}
+
 // ====================================================== p planes
 // p = M(t)^-1 grad(phi), M = I + t grad grad phi (lense_flow.py:373-381,
 // :398-415), at the K = 2n+1 stage times t_k = t0 + k hh of an RK4

@@ -364,6 +364,14 @@ def lense_flow_ad(f, phi, pix_width, n=10, direction=FORWARD_LENSE, precision="f
     return LenseFlowFunction.apply(f, phi, pix_width, n, direction, precision)
 
 
+def wait_timeouts(reset=False):
+    """1 if a kernel block gave up waiting for its bulk copies since the last reset (its results are invalid)."""
+    import ctypes
+    count = ctypes.c_int(0)
+    nat.check(nat.load().lf_wait_timeouts(ctypes.byref(count), int(bool(reset))), "lf_wait_timeouts")
+    return count.value
+
+
 def get_plan(nside, ncomp, pix_width, precision="f32", device=None):
     dev = torch.cuda.current_device() if device is None else torch.device(device).index
     key = (dev, int(nside), int(ncomp), float(pix_width), precision)

@@ -149,6 +149,13 @@ int lf_lense_flow_noalloc(int nside, int ncomp, double pix_width, const void* f_
  * lf_profile_read synchronises on the last event and returns the summed
  * duration and count of the recorded launches of one kind.  No counterpart
  * in the reference (its device work is XLA-generated). */
+/* Set to 1 (and kept) if a kernel block stopped waiting for its own bulk
+ * copies into shared memory after its bounded number of polls; that block
+ * skipped its work, so results computed since the last reset are invalid.
+ * Synchronises the current device.  No counterpart in the reference (its
+ * XLA path has no device-side waits). */
+int lf_wait_timeouts(int* count, int reset);
+
 enum lf_kernel_kind { LF_KIND_ROW = 0, LF_KIND_COL = 1, LF_KIND_PHI = 2, LF_KIND_PP = 3 };
 int lf_profile_enable(lf_plan_t plan, int enable);
 int lf_profile_reset(lf_plan_t plan);

@@ -84,6 +84,19 @@ def test_p_plane_and_derivative_plane_paths(torch_cuda, C, direction, adjoint):
     assert rel_l2(outs[0], outs[1]) < 1e-6
 
 
+def test_qu512_stage_waits_complete(torch_cuda):
+    """The 512^2 QU stage kernel stages its operands with bulk copies; every block's bounded wait completes."""
+    import torch
+    from cmblensing_b200 import engine
+    engine.wait_timeouts(reset=True)
+    f, phis = _inputs(512, 2.0, 2, B=3, seed0=9)
+    pw = R.pix_width_of(2.0)
+    for direction in (1, -1):
+        _engine(torch, f, phis, pw, 7, direction, False)
+    torch.cuda.synchronize()
+    assert engine.wait_timeouts() == 0
+
+
 def test_lens_1024_T(torch_cuda):
     f, phis = _inputs(1024, 2.0, 1)
     pw = R.pix_width_of(2.0)
