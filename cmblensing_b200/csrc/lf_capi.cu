@@ -40,7 +40,24 @@ struct lf_plan_s {
   int device;
   void* tw;        // N complex values in the compute precision
   double2* tw64;   // N complex float64 (phi precompute)
+  void* twp;       // pass table of length N in the compute precision
 };
+
+// Pass table of length L (layout: ptw_offset / ptw_size): store(i, cos, sin)
+// for every entry, values computed in float64.
+template <class Store>
+static void fill_pass_table(int L, Store store) {
+  for (int b = 0; b < 4; ++b) {
+    const PtwBlock x = ptw_candidate(L, b);
+    if (x.R == 0 || ptw_repeats(L, b)) continue;
+    const int off = ptw_offset(L, x.R, x.NS);
+    for (int r = 1; r < x.R; ++r)
+      for (int k = 0; k < x.NS; ++k) {
+        const double ang = -2.0 * M_PI * (double)r * (double)k / ((double)x.R * (double)x.NS);
+        store(off + (r - 1) * x.NS + k, std::cos(ang), std::sin(ang));
+      }
+  }
+}
 
 namespace {
 
@@ -125,7 +142,7 @@ cudaError_t run_lens_pp(const StageArgs& base, int B, int nsteps, double t0, dou
   constexpr int RMB = Geo<T>::row_minb(N);
   constexpr int H = N / 2;
   const size_t smem_row = sizeof(c2<T>) * (N + 2 * C * RL * H);
-  const size_t smem_col = sizeof(c2<T>) * (N + LINES * N);
+  const size_t smem_col = sizeof(c2<T>) * (col_tw_entries(N) + LINES * N);
   const dim3 grow(N / RL, B);
   const dim3 gcol(H / LINES, B * C);
   StageArgs a = base;
@@ -343,7 +360,7 @@ cudaError_t run_vjp_n(const StageArgs& af0, const StageArgs& ad0, double* dacc, 
   constexpr int RMB = Geo<T>::row_minb(N);
   constexpr int H = N / 2;
   const size_t smem_row = sizeof(c2<T>) * (N + 2 * C * RL * H);
-  const size_t smem_col = sizeof(c2<T>) * (N + LINES * N);
+  const size_t smem_col = sizeof(c2<T>) * (col_tw_entries(N) + LINES * N);
   const dim3 grow(N / RL, B);
   const dim3 gcol(H / LINES, B * C);
   const long P = (long)N * N;
@@ -460,6 +477,20 @@ int lf_plan_create(lf_plan_t* out, int nside, int ncomp, double pix_width, int p
       if (e == cudaSuccess) e = cudaMemcpy(p->tw, t32.data(), sizeof(float2) * nside, cudaMemcpyHostToDevice);
     }
   }
+  if (e == cudaSuccess) {
+    const size_t np = (size_t)ptw_size(nside);
+    std::vector<double2> pt(np);
+    std::vector<float2> pt32(np);
+    fill_pass_table(nside, [&](int i, double c, double sn) {
+      pt[i] = make_double2(c, sn);
+      pt32[i] = make_float2((float)c, (float)sn);
+    });
+    const bool f64 = precision == LF_F64;
+    const size_t bytes = f64 ? sizeof(double2) * np : sizeof(float2) * np;
+    e = cudaMalloc(&p->twp, bytes);
+    if (e == cudaSuccess)
+      e = cudaMemcpy(p->twp, f64 ? (const void*)pt.data() : (const void*)pt32.data(), bytes, cudaMemcpyHostToDevice);
+  }
   if (e != cudaSuccess) {
     lf_plan_destroy(p);
     return cuda_status(e);
@@ -472,6 +503,7 @@ int lf_plan_destroy(lf_plan_t p) {
   if (!p) return LF_OK;
   if (p->tw && p->tw != p->tw64) cudaFree(p->tw);
   if (p->tw64) cudaFree(p->tw64);
+  if (p->twp) cudaFree(p->twp);
   for (cudaEvent_t e : p->prof.pool) cudaEventDestroy(e);
   delete p;
   return LF_OK;
@@ -580,6 +612,7 @@ int lf_lense_flow(lf_plan_t p, const void* f_in, int in_dtype, void* f_out, int 
   const size_t ppb = pp_bytes(p, batch, nsteps);
   if (ppb && ws_bytes >= base_bytes + ppb) a.pp = w + base_bytes;
   a.twN = p->tw;
+  a.twP = p->twp;
   a.kbase = 2.0 * M_PI / ((double)p->N * p->pix_width);
   a.nplanes = batch * p->C;
   cudaError_t e;
@@ -676,6 +709,7 @@ int lf_lense_flow_vjp(lf_plan_t p, const void* f_lensed, const void* cotangent, 
   af.s = fs + 2 * plane;
   af.gx = fs + 3 * plane;
   af.twN = p->tw;
+  af.twP = p->twp;
   af.kbase = 2.0 * M_PI / ((double)p->N * p->pix_width);
   af.nplanes = batch * p->C;
   af.grad = grad;
@@ -752,6 +786,9 @@ int lf_profile_read(lf_plan_t p, int kind, double* total_ms, int* launches) {
 // on the first call on the device, and only those addresses reach kernels.
 static __device__ __align__(256) unsigned char g_noalloc_scratch[LF_NOALLOC_SCRATCH_BYTES];
 static __device__ __align__(256) float2 g_noalloc_tw[64 + 128 + 256 + 512 + 1024];
+// pass tables (column pass) of every supported N, back to back
+constexpr int kNoAllocTwp = ptw_size(64) + ptw_size(128) + ptw_size(256) + ptw_size(512) + ptw_size(1024);
+static __device__ __align__(256) float2 g_noalloc_twp[kNoAllocTwp];
 
 namespace {
 
@@ -759,6 +796,7 @@ struct NoAllocDevice {
   bool ready = false;
   char* scratch = nullptr;  // device address of g_noalloc_scratch
   float2* tw = nullptr;     // device address of g_noalloc_tw
+  float2* twp = nullptr;    // device address of g_noalloc_twp
 };
 
 constexpr int kNoAllocMaxDevices = 64;
@@ -767,6 +805,12 @@ std::mutex g_noalloc_mu;
 
 int noalloc_tw_offset(int n) {
   return n == 64 ? 0 : n == 128 ? 64 : n == 256 ? 192 : n == 512 ? 448 : 960;
+}
+
+int noalloc_twp_offset(int n) {
+  int off = 0;
+  for (int m = 64; m < n; m *= 2) off += ptw_size(m);
+  return off;
 }
 
 // Once per device: resolve the arrays' device addresses and fill the twiddle
@@ -796,8 +840,19 @@ int noalloc_setup(NoAllocDevice** out) {
     }
     e = cudaMemcpyToSymbol(g_noalloc_tw, host, sizeof(host));
     if (e != cudaSuccess) return cuda_status(e);
+    void* twp = nullptr;
+    e = cudaGetSymbolAddress(&twp, g_noalloc_twp);
+    if (e != cudaSuccess) return cuda_status(e);
+    static float2 host_p[kNoAllocTwp];
+    for (int n = 64; n <= 1024; n *= 2) {
+      const int off = noalloc_twp_offset(n);
+      fill_pass_table(n, [&](int i, double c, double sn) { host_p[off + i] = make_float2((float)c, (float)sn); });
+    }
+    e = cudaMemcpyToSymbol(g_noalloc_twp, host_p, sizeof(host_p));
+    if (e != cudaSuccess) return cuda_status(e);
     d.scratch = reinterpret_cast<char*>(scratch);
     d.tw = reinterpret_cast<float2*>(tw);
+    d.twp = reinterpret_cast<float2*>(twp);
     d.ready = true;
   }
   *out = &d;
@@ -844,6 +899,7 @@ extern "C" int lf_lense_flow_noalloc(int nside, int ncomp, double pix_width, con
   a.gx = d->scratch + 3 * plane_bytes;
   a.v = adj ? (void*)(d->scratch + 4 * plane_bytes) : nullptr;
   a.twN = d->tw + noalloc_tw_offset(nside);
+  a.twP = d->twp + noalloc_twp_offset(nside);
   a.kbase = 2.0 * M_PI / ((double)nside * pix_width);
   a.nplanes = batch * ncomp;
   g_prof = nullptr;

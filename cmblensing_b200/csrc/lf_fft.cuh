@@ -152,6 +152,61 @@ template <typename T, int LINES> __device__ __forceinline__ int sw(int m, int li
   }
 }
 
+// ------------------------------------------------------- plans and tables
+// Radices of the length-L plan: R1 x R2 (x R3).  The inverse half of
+// fft_mul_ifft runs them in reverse order.
+__host__ __device__ constexpr int plan_r1(int L) { return (L == 256 || L == 1024) ? 16 : 8; }
+__host__ __device__ constexpr int plan_r2(int L) { return L == 32 ? 4 : (L == 64 || L == 512 || L == 1024) ? 8 : 16; }
+__host__ __device__ constexpr int plan_r3(int L) { return (L == 512 || L == 1024) ? 8 : 1; }
+
+// Pass twiddle tables.  A pass of radix R after passes of total length NS
+// multiplies input r of butterfly j by W_{R NS}^{r k}, k = j mod NS.  Read
+// from one table tw[r k NTAB / (R NS)], the threads of a warp (consecutive k)
+// hit addresses r NTAB / (R NS) apart -- the same bank for many of them.  A
+// pass table stores W^{r k} at (r - 1) NS + k instead, so a warp's reads are
+// consecutive.  The table of length L holds one block per distinct (R, NS)
+// of the forward plan and of the reversed (inverse) plan.
+struct PtwBlock {
+  int R, NS;
+};
+
+__host__ __device__ constexpr PtwBlock ptw_candidate(int L, int b) {
+  const int r1 = plan_r1(L), r2 = plan_r2(L), r3 = plan_r3(L);
+  if (r3 > 1)  // forward (r2, r1), (r3, r1 r2); reversed (r2, r3), (r1, r3 r2)
+    return b == 0 ? PtwBlock{r2, r1} : b == 1 ? PtwBlock{r3, r1 * r2} : b == 2 ? PtwBlock{r2, r3} : PtwBlock{r1, r3 * r2};
+  return b == 0 ? PtwBlock{r2, r1} : b == 1 ? PtwBlock{r1, r2} : PtwBlock{0, 0};  // forward, reversed
+}
+
+__host__ __device__ constexpr bool ptw_repeats(int L, int b) {
+  for (int c = 0; c < b; ++c) {
+    const PtwBlock x = ptw_candidate(L, c), y = ptw_candidate(L, b);
+    if (x.R == y.R && x.NS == y.NS) return true;
+  }
+  return false;
+}
+
+// offset of the (R, NS) block in the pass table of length L (-1: none)
+__host__ __device__ constexpr int ptw_offset(int L, int R, int NS) {
+  int off = 0;
+  for (int b = 0; b < 4; ++b) {
+    const PtwBlock x = ptw_candidate(L, b);
+    if (x.R == 0 || ptw_repeats(L, b)) continue;
+    if (x.R == R && x.NS == NS) return off;
+    off += (x.R - 1) * x.NS;
+  }
+  return -1;
+}
+
+__host__ __device__ constexpr int ptw_size(int L) {
+  int off = 0;
+  for (int b = 0; b < 4; ++b) {
+    const PtwBlock x = ptw_candidate(L, b);
+    if (x.R == 0 || ptw_repeats(L, b)) continue;
+    off += (x.R - 1) * x.NS;
+  }
+  return off;
+}
+
 // ------------------------------------------------------------ Stockham pass
 // One radix-R pass over the LINES lines of NTILES consecutive tiles
 // (TILE_ELEMS apart) of length L.  NS is the product of the radices of the
@@ -162,7 +217,9 @@ struct NoPre {
   template <typename V> __device__ __forceinline__ V operator()(int, int, int, V v) const { return v; }
 };
 
-template <typename T, int L, int R, int NS, int LINES, int NTILES, int NT, bool INV, int NTAB, class Pre = NoPre>
+// PT: ``tw`` points at this pass's block of a pass table (see ptw_offset).
+template <typename T, int L, int R, int NS, int LINES, int NTILES, int NT, bool INV, int NTAB, bool PT = false,
+          class Pre = NoPre>
 __device__ __forceinline__ void stockham_pass(c2<T>* __restrict__ buf, const c2<T>* __restrict__ tw, int tid,
                                               Pre pre = Pre()) {
   constexpr int NB = L / R;                   // butterflies per line
@@ -186,7 +243,7 @@ __device__ __forceinline__ void stockham_pass(c2<T>* __restrict__ buf, const c2<
       if constexpr (NS > 1) {
         const int k = j % NS;
 #pragma unroll
-        for (int r = 1; r < R; ++r) v[b][r] = twmul<T, INV>(v[b][r], tw[r * k * TWS]);
+        for (int r = 1; r < R; ++r) v[b][r] = twmul<T, INV>(v[b][r], PT ? tw[(r - 1) * NS + k] : tw[r * k * TWS]);
       }
       dft<R, T, INV>(v[b]);
     }
@@ -254,7 +311,7 @@ template <int L, int R, int LINES, int NT> struct SpGeom {
   static constexpr int PER = (TOT + NT - 1) / NT;
 };
 
-template <typename T, int L, int R, int NS, int LINES, int NT, bool INV, int NTAB, class Src>
+template <typename T, int L, int R, int NS, int LINES, int NT, bool INV, int NTAB, bool PT, class Src>
 __device__ __forceinline__ void sp_read(c2<T> (&v)[SpGeom<L, R, LINES, NT>::PER][R], Src src,
                                         const c2<T>* tw, int tid) {
   using G = SpGeom<L, R, LINES, NT>;
@@ -270,7 +327,7 @@ __device__ __forceinline__ void sp_read(c2<T> (&v)[SpGeom<L, R, LINES, NT>::PER]
       if constexpr (NS > 1) {
         const int k = j % NS;
 #pragma unroll
-        for (int r = 1; r < R; ++r) v[b][r] = twmul<T, INV>(v[b][r], tw[r * k * TWS]);
+        for (int r = 1; r < R; ++r) v[b][r] = twmul<T, INV>(v[b][r], PT ? tw[(r - 1) * NS + k] : tw[r * k * TWS]);
       }
       dft<R, T, INV>(v[b]);
     }
@@ -313,22 +370,26 @@ __device__ __forceinline__ void sp_write(c2<T>* buf, c2<T> (&v)[SpGeom<L, R, LIN
 // ``dst(m, line, x)``, so shared memory sees 2 * (passes - 1) sweeps instead
 // of 2 * (2 passes + 1).  ``mul(m, line, x)`` gets the spectrum at frequency m.
 // Plans: 32 = 8x4, 64 = 8x8, 128 = 8x16, 256 = 16x16, 512 = 8x8x8, 1024 = 16x8x8.
-template <typename T, int L, int LINES, int NT, int NTAB, class Src, class Mul, class Dst>
+// ``tw`` is the pass table of length L (ptw_size(L) entries).
+template <typename T, int L, int LINES, int NT, class Src, class Mul, class Dst>
 __device__ __forceinline__ void fft_mul_ifft(c2<T>* buf, const c2<T>* tw, int tid, Src src, Mul mul,
                                              Dst dst) {
   auto smem = [=](int m, int line) { return buf[sw<T, LINES>(m, line)]; };
-  constexpr int R1 = (L == 32 || L == 64 || L == 128 || L == 512) ? 8 : 16;
-  constexpr int R2 = (L == 32) ? 4 : (L == 64 || L == 512 || L == 1024) ? 8 : 16;
-  constexpr int R3 = (L == 512 || L == 1024) ? 8 : 1;
+  constexpr int R1 = plan_r1(L), R2 = plan_r2(L), R3 = plan_r3(L);
+  // pass-table blocks (``tw`` is the pass table of length L); first passes read no twiddles
+  constexpr int OF2 = ptw_offset(L, R2, R1), OF3 = ptw_offset(L, R3, R1 * R2);
+  constexpr int OI2 = ptw_offset(L, R3 == 1 ? R1 : R2, R3 == 1 ? R2 : R3);
+  constexpr int OI3 = ptw_offset(L, R1, R3 * R2);
+  static_assert(OF2 >= 0 && OI2 >= 0 && (R3 == 1 || (OF3 >= 0 && OI3 >= 0)), "pass table block missing");
   static_assert(L == 32 || L == 64 || L == 128 || L == 256 || L == 512 || L == 1024, "unsupported length");
   if constexpr (R3 == 1) {
     static_assert(R1 * R2 == L, "plan");
     c2<T> a[SpGeom<L, R1, LINES, NT>::PER][R1];
     c2<T> b[SpGeom<L, R2, LINES, NT>::PER][R2];
-    sp_read<T, L, R1, 1, LINES, NT, false, NTAB>(a, src, tw, tid);
+    sp_read<T, L, R1, 1, LINES, NT, false, L, true>(a, src, tw, tid);
     sp_write<T, L, R1, 1, LINES, NT>(buf, a, tid);
     __syncthreads();
-    sp_read<T, L, R2, R1, LINES, NT, false, NTAB>(b, smem, tw, tid);
+    sp_read<T, L, R2, R1, LINES, NT, false, L, true>(b, smem, tw + OF2, tid);
     sp_apply<T, L, R2, R1, LINES, NT>(b, mul, tid);
 #pragma unroll
     for (int i = 0; i < SpGeom<L, R2, LINES, NT>::PER; ++i) {
@@ -338,21 +399,21 @@ __device__ __forceinline__ void fft_mul_ifft(c2<T>* buf, const c2<T>* tw, int ti
     __syncthreads();
     sp_write<T, L, R2, 1, LINES, NT>(buf, b, tid);
     __syncthreads();
-    sp_read<T, L, R1, R2, LINES, NT, true, NTAB>(a, smem, tw, tid);
+    sp_read<T, L, R1, R2, LINES, NT, true, L, true>(a, smem, tw + OI2, tid);
     sp_emit<T, L, R1, R2, LINES, NT>(a, dst, tid);
   } else {
     static_assert(R1 * R2 * R3 == L, "plan");
     c2<T> a[SpGeom<L, R1, LINES, NT>::PER][R1];
     c2<T> b[SpGeom<L, R2, LINES, NT>::PER][R2];
     c2<T> c[SpGeom<L, R3, LINES, NT>::PER][R3];
-    sp_read<T, L, R1, 1, LINES, NT, false, NTAB>(a, src, tw, tid);
+    sp_read<T, L, R1, 1, LINES, NT, false, L, true>(a, src, tw, tid);
     sp_write<T, L, R1, 1, LINES, NT>(buf, a, tid);
     __syncthreads();
-    sp_read<T, L, R2, R1, LINES, NT, false, NTAB>(b, smem, tw, tid);
+    sp_read<T, L, R2, R1, LINES, NT, false, L, true>(b, smem, tw + OF2, tid);
     __syncthreads();
     sp_write<T, L, R2, R1, LINES, NT>(buf, b, tid);
     __syncthreads();
-    sp_read<T, L, R3, R1 * R2, LINES, NT, false, NTAB>(c, smem, tw, tid);
+    sp_read<T, L, R3, R1 * R2, LINES, NT, false, L, true>(c, smem, tw + OF3, tid);
     sp_apply<T, L, R3, R1 * R2, LINES, NT>(c, mul, tid);
 #pragma unroll
     for (int i = 0; i < SpGeom<L, R3, LINES, NT>::PER; ++i) {
@@ -362,11 +423,11 @@ __device__ __forceinline__ void fft_mul_ifft(c2<T>* buf, const c2<T>* tw, int ti
     __syncthreads();
     sp_write<T, L, R3, 1, LINES, NT>(buf, c, tid);
     __syncthreads();
-    sp_read<T, L, R2, R3, LINES, NT, true, NTAB>(b, smem, tw, tid);
+    sp_read<T, L, R2, R3, LINES, NT, true, L, true>(b, smem, tw + OI2, tid);
     __syncthreads();
     sp_write<T, L, R2, R3, LINES, NT>(buf, b, tid);
     __syncthreads();
-    sp_read<T, L, R1, R3 * R2, LINES, NT, true, NTAB>(a, smem, tw, tid);
+    sp_read<T, L, R1, R3 * R2, LINES, NT, true, L, true>(a, smem, tw + OI3, tid);
     sp_emit<T, L, R1, R3 * R2, LINES, NT>(a, dst, tid);
   }
 }

@@ -38,6 +38,7 @@ struct StageArgs {
   void* v;   // adjoint: V = rfft_rows(p_y y_s)
   void* gx;  // column pass output
   const void* twN;  // N complex T, exp(-2 pi i k / N)
+  const void* twP;  // pass table of length N (ptw_size(N) complex T): column pass, paired row pass
   double kbase;     // 2 pi / (N d)
   double t_cur;     // time of the rate evaluated in this stage
   double t_next;    // time of the next stage input
@@ -113,6 +114,10 @@ __device__ __forceinline__ void load_twiddles(c2<T>* tw, const void* g, int tid)
   for (int i = tid; i < N; i += NT) tw[i] = src[i];
 }
 
+// shared-memory entries reserved for the column pass's pass table (rounded
+// up to an even count so that the tile after it stays 16-byte aligned)
+__host__ __device__ constexpr int col_tw_entries(int n) { return (ptw_size(n) + 1) & ~1; }
+
 // ======================================================== column pass
 // Gx = IFFT_col( (i KX / N^2) * FFT_col(S) ) on tiles of LINES columns.
 // grid: x = column tile (N/2/LINES), y = plane.
@@ -120,13 +125,13 @@ template <typename T, int N, int LINES, int NT, int MINB = 1>
 __global__ void __launch_bounds__(NT, MINB) k_col(StageArgs a) {
   constexpr int H = N / 2;
   extern __shared__ __align__(16) unsigned char smem_raw[];
-  c2<T>* tw = reinterpret_cast<c2<T>*>(smem_raw);
-  c2<T>* buf = tw + N;
+  c2<T>* tw = reinterpret_cast<c2<T>*>(smem_raw);  // pass table
+  c2<T>* buf = tw + col_tw_entries(N);
   const int tid = threadIdx.x;
   const int c0 = blockIdx.x * LINES;
   const long plane = blockIdx.y;
   static_assert(H % LINES == 0, "column tiles must cover the packed spectrum");
-  load_twiddles<T, N, NT>(tw, a.twN, tid);
+  load_twiddles<T, ptw_size(N), NT>(tw, a.twP, tid);
   const c2<T>* in = reinterpret_cast<const c2<T>*>(a.s) + plane * (long)N * H + c0;
   c2<T>* out = reinterpret_cast<c2<T>*>(a.gx) + plane * (long)N * H + c0;
   // i KX / N^2 between the transforms; zero on KX's Nyquist row of the packed
@@ -140,7 +145,7 @@ __global__ void __launch_bounds__(NT, MINB) k_col(StageArgs a) {
   // rows of LINES consecutive columns: each warp's accesses cover whole 128-byte lines
   auto src = [=](int m, int line) { return in[m * H + line]; };
   auto dst = [=](int m, int line, c2<T> x) { out[m * H + line] = x; };
-  fft_mul_ifft<T, N, LINES, NT, N>(buf, tw, tid, src, kx_mul, dst);
+  fft_mul_ifft<T, N, LINES, NT>(buf, tw, tid, src, kx_mul, dst);
 }
 
 // ========================================================= row pass
@@ -450,7 +455,9 @@ __global__ void __launch_bounds__(NT, MINB) k_row_pair(StageArgs a) {
       bulk_g2s(stg + (4 + c) * RB, pp + c * P, RB * sizeof(T), mbar);
     }
   }
-  load_twiddles<T, N, NT>(tw, a.twN, tid);
+  load_twiddles<T, ptw_size(N), NT>(tw, a.twP, tid);  // pass table (fits the N entries reserved)
+  static_assert(ptw_size(N) <= N, "pass table of the 8x8x8 plan");
+  constexpr int O8 = ptw_offset(N, R, R), O64 = ptw_offset(N, R, R * R);
   const T ky_scale = T(a.kbase / double(N));
   const long half_plane = N * (long)H;
   auto spec = [&](void* base, int c) {
@@ -484,8 +491,8 @@ __global__ void __launch_bounds__(NT, MINB) k_row_pair(StageArgs a) {
     }
   }
   __syncthreads();
-  stockham_pass<T, N, R, 1, LINES, 2, NT, true, N>(buf, tw, tid);
-  stockham_pass<T, N, R, R, LINES, 2, NT, true, N>(buf, tw, tid);
+  stockham_pass<T, N, R, 1, LINES, 2, NT, true, N, true>(buf, tw, tid);
+  stockham_pass<T, N, R, R, LINES, 2, NT, true, N, true>(buf, tw + O8, tid);
 
   // ----------------- inverse pass 3 -> RK4 update -> forward pass 1, in registers
   const int j = tid % NB, row = tid / NB;
@@ -497,7 +504,7 @@ __global__ void __launch_bounds__(NT, MINB) k_row_pair(StageArgs a) {
   }
 #pragma unroll
   for (int r = 1; r < R; ++r) {
-    const c2<T> w = tw[r * j];  // W_N^(r j): NS = N / R
+    const c2<T> w = tw[O64 + (r - 1) * NB + j];  // W_N^(r j): NS = N / R
 #pragma unroll
     for (int c = 0; c < 2; ++c) v[c][r] = twmul<T, true>(v[c][r], w);
   }
@@ -554,8 +561,8 @@ __global__ void __launch_bounds__(NT, MINB) k_row_pair(StageArgs a) {
 #pragma unroll
   for (int r = 0; r < R; ++r) buf[sw<T, LINES>(R * j + r, row)] = w[r];
   __syncthreads();
-  stockham_pass<T, N, R, R, LINES, 1, NT, false, N>(buf, tw, tid);
-  stockham_pass<T, N, R, R * R, LINES, 1, NT, false, N>(buf, tw, tid);
+  stockham_pass<T, N, R, R, LINES, 1, NT, false, N, true>(buf, tw + O8, tid);
+  stockham_pass<T, N, R, R * R, LINES, 1, NT, false, N, true>(buf, tw + O64, tid);
 
   // ------------------------------ split W into the two packed row spectra
 #pragma unroll
