@@ -29,3 +29,13 @@ def logpdf(field, phi, data, noise_covariance, phi_covariance, field_covariance,
     resid = data - mask * beam * lensed
     like = dot(resid, pinv(noise_covariance) * resid)
     return -_real(like + prior_f + prior_phi + logdets) / 2
+
+
+@on_device
+def mixed_logpdf(mixed_field, mixed_phi, data, noise_covariance, phi_covariance, field_covariance, mask, beam,
+                 mixing_g, mixing_d, n=10):
+    """statistics.py:168-181: logpdf at unmix(f_mixed, phi_mixed) minus Re log det G and Re log det D."""
+    from .mixing import unmix
+    field, phi = unmix.__wrapped__(mixed_field, mixed_phi, mixing_d, mixing_g, n=n)
+    value = logpdf.__wrapped__(field, phi, data, noise_covariance, phi_covariance, field_covariance, mask, beam, n=n)
+    return value - _real(log_det(mixing_g)) - _real(log_det(mixing_d))

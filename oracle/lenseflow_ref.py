@@ -765,3 +765,82 @@ def wiener_filter(field, phi, data, field_covariance, noise_covariance, mask, be
         return gradf_logpdf(f, phi, f * 0, field_covariance, noise_covariance, mask, beam, n=n)
 
     return conjugate_gradient(field, apply_A, b, P, maxiter=maxiter, tol=tol, rel_tol=rel_tol)
+
+
+# --------------------------------------------------- simulation and sampling
+def field_from_normals(nside, covar_matrix, real_normals, imag_normals):
+    """simulate.py:106-113 with the two normal draws given: irfft2(sqrt(C/2) (a + i b), norm="ortho")."""
+    field = np.sqrt(np.asarray(covar_matrix) / 2) * (real_normals + 1j * imag_normals)
+    return np.fft.irfft2(field, s=(nside, nside), norm="ortho")
+
+
+def mixed_logpdf(mixed_field, mixed_phi, data, noise_covariance, phi_covariance, field_covariance, mask, beam,
+                 mixing_g, mixing_d, n=10):
+    """statistics.py:168-181: logpdf at the unmixed point minus Re log det G and Re log det D."""
+    field, phi = unmix(mixed_field, mixed_phi, mixing_d, mixing_g, n=n)
+    value = logpdf(field, phi, data, noise_covariance, phi_covariance, field_covariance, mask, beam, n=n)
+    return value - np.real(log_det(mixing_g)) - np.real(log_det(mixing_d))
+
+
+def get_mass_matrix(cphi, nphi, mixing_g):
+    """sampling_ar.py:65-66: G^-1 G^-1 (Cphi^-1 + Nphi^-1)."""
+    return pinv(mixing_g) * pinv(mixing_g) * (pinv(cphi) + pinv(nphi))
+
+
+def symplectic_integrate(x0, p0, mixed_field, data, noise_covariance, phi_covariance, field_covariance, mask, beam,
+                         mixing_d, mixing_g, mass_matrix, num_steps=30, step_size=0.01, n=10):
+    """sampling_ar.py:104-135: the reference's leapfrog (gradient of +logpdf) and delta H."""
+    def grad(x):
+        return x.replace(scalar_matrix=mixed_grad_phi_logpdf(mixed_field, x, data, noise_covariance, phi_covariance,
+                                                             field_covariance, mask, beam, mixing_d, mixing_g, n=n))
+
+    def hamiltonian(x, p):
+        lp = mixed_logpdf(mixed_field, x, data, noise_covariance, phi_covariance, field_covariance, mask, beam,
+                          mixing_g, mixing_d, n=n)
+        return lp - dot(p, (pinv(mass_matrix) * p) / 2)
+
+    minv = pinv(mass_matrix)
+    g = grad(x0)
+    x, p = x0, p0
+    for _ in range(num_steps):
+        prev = g
+        x = x - step_size * (minv * (p - 0.5 * step_size * g))
+        g = grad(x)
+        p = p - 0.5 * step_size * (g + prev)
+    return hamiltonian(x, p) - hamiltonian(x0, p0), x, p
+
+
+def hmc_step_from_draws(x, always_accept, mass_matrix, p_real, p_imag, log_u, mixed_field, data, noise_covariance,
+                        phi_covariance, field_covariance, mask, beam, mixing_d, mixing_g, num_steps=30,
+                        step_size=0.01, n=10):
+    """sampling_ar.py:69-100 with the momentum normals and log(uniform) given.
+
+    The momentum is a FlatS0 with the mixed field's Fourier weights (the
+    reference writes it through ``mixed_field.replace(scalar_matrix=...)``).
+    """
+    nside = x.nside
+    p = FlatS0(scalar_matrix=np.fft.rfft2(field_from_normals(nside, mass_matrix.scalar_matrix, p_real, p_imag)),
+               fourier_weights=mixed_field.fourier_weights)
+    delta_h, x_test, _ = symplectic_integrate(x, p, mixed_field, data, noise_covariance, phi_covariance,
+                                              field_covariance, mask, beam, mixing_d, mixing_g, mass_matrix,
+                                              num_steps=num_steps, step_size=step_size, n=n)
+    accept = bool(always_accept or (log_u < delta_h))
+    return (x_test if accept else x), delta_h, accept
+
+
+def gibbs_sample_f_from_draws(field_start, data, phi, field_covariance, noise_covariance, mask, beam, f_draws,
+                              n_draws, n=10, maxiter=500, tol=1e-1):
+    """sampling_ar.py:15-46 for a T field with the two normal pairs given.
+
+    f' = f_sim + WF(d - (M B L f_sim + n_sim)): a constrained realisation.
+    """
+    nside = data.nside
+    new_field = field_start.replace(scalar_matrix=np.fft.rfft2(
+        field_from_normals(nside, field_covariance.scalar_matrix, *f_draws)))
+    new_noise = field_start.replace(scalar_matrix=np.fft.rfft2(
+        field_from_normals(nside, noise_covariance.scalar_matrix, *n_draws)))
+    lensed = qu2eb(fourier(lense_flow(map_(eb2qu(new_field)), map_(phi), n=n)))
+    new_data = mask * beam * lensed + new_noise
+    delta, _ = wiener_filter(field_start, phi, data - new_data, field_covariance, noise_covariance, mask, beam, n=n,
+                             maxiter=maxiter, tol=tol)
+    return new_field + delta
