@@ -844,3 +844,62 @@ def gibbs_sample_f_from_draws(field_start, data, phi, field_covariance, noise_co
     delta, _ = wiener_filter(field_start, phi, data - new_data, field_covariance, noise_covariance, mask, beam, n=n,
                              maxiter=maxiter, tol=tol)
     return new_field + delta
+
+
+# ---------------------------------------------------------------- MAP joint
+def get_scalar_identity(op):
+    """matrix_operators.py:159-170."""
+    shape = (op.nside, op.nside // 2 + 1)
+    return DiagonalScalar(fourier_weights=get_fourier_weights(shape), nside=op.nside, theta_pix=op.theta_pix,
+                          pix_width=op.pix_width, scalar_matrix=np.ones(shape, dtype=np.complex128))
+
+
+def zero_scalar_field_like(field):
+    """fields.py:123-133."""
+    shape = (field.nside, field.nside // 2 + 1)
+    return FlatS0(fourier_weights=get_fourier_weights(shape), nside=field.nside, theta_pix=field.theta_pix,
+                  pix_width=field.pix_width, scalar_matrix=np.zeros(shape, dtype=np.complex128))
+
+
+def phi_gradient_hessian(phi_covariance, quadratic_estimate):
+    """map_joint.py:72-77: Cphi^-1 + Nphi^-1."""
+    return pinv(phi_covariance) + pinv(quadratic_estimate)
+
+
+def logpdf_at_phi_new(alpha, grad_phi, mixed_field, phi_predict, data, beam, mask, field_covariance, phi_covariance,
+                      noise_covariance, mixing_d, mixing_g, hessian, n=10):
+    """map_joint.py:79-98: -logpdf at unmix(f_mixed, phi + alpha H^-1 grad)."""
+    test_phi = phi_predict + alpha * (hessian * grad_phi)
+    field, phi = unmix(mixed_field, test_phi, mixing_d, mixing_g, n=n)
+    return -logpdf(field, phi, data, noise_covariance, phi_covariance, field_covariance, mask, beam, n=n)
+
+
+def map_joint(data, noise_covariance, mixing_d, field_covariance, phi_covariance, quadratic_estimate, mask, beam,
+              num_steps=30, constant_step=False, n=10, wf_maxiter=500, wf_tol=1e-1):
+    """map_joint.py:19-67 with the data set's members passed one by one.
+
+    Each step: Wiener-filter f at the current phi (reference rule), mix with
+    G = 1, the mixed phi gradient, a scipy BFGS search for the step length
+    alpha (from 1; alpha = 1 throughout with ``constant_step``) and
+    phi <- phi + alpha H^-1-preconditioned gradient, H = Cphi^-1 + Nphi^-1.
+    """
+    from scipy.optimize import minimize
+    mixing_g = get_scalar_identity(mixing_d)
+    field = data * 0
+    phi = zero_scalar_field_like(data)
+    hessian = pinv(phi_gradient_hessian(phi_covariance, quadratic_estimate))
+    alpha = 1.0
+    for _ in range(num_steps):
+        field, _ = wiener_filter(field, phi, data, field_covariance, noise_covariance, mask, beam, n=n,
+                                 maxiter=wf_maxiter, tol=wf_tol)
+        mixed_field, mixed_phi = mix(field, phi, mixing_d, mixing_g, n=n)
+        grad = mixed_phi.replace(scalar_matrix=mixed_grad_phi_logpdf(
+            mixed_field, mixed_phi, data, noise_covariance, phi_covariance, field_covariance, mask, beam, mixing_d,
+            mixing_g, n=n))
+        if not constant_step:
+            f = lambda a: logpdf_at_phi_new(float(np.asarray(a).ravel()[0]), grad, mixed_field, mixed_phi, data,
+                                            beam, mask, field_covariance, phi_covariance, noise_covariance,
+                                            mixing_d, mixing_g, hessian, n=n)
+            alpha = float(minimize(f, 1.0, method="BFGS").x[0])
+        phi = phi + alpha * (hessian * grad)
+    return field, phi

@@ -11,8 +11,9 @@ this script:
   subsample of 8192 entries plus the row/column indices, so the fixtures stay
   small while still pinning every output;
 * logpdf scalars are stored exactly;
-* ``mix.npz`` holds the mixing diagonals D (T, EE, BB) and G with the
-  subsampled mixed phi gradients (T-only and QU-only sets).
+* ``mix.npz`` holds the mixing diagonals D (T, EE, BB) and G, the
+  quadratic-estimate noise Nphi (T and QU sets) and the subsampled mixed phi
+  gradients (T-only and QU-only sets).
 
 Run once in a container that has the reference checked out::
 
@@ -75,6 +76,7 @@ def main(src):
     # mixed parametrisation: mixing diagonals D, G in full, mixed phi gradients subsampled
     np.savez_compressed(os.path.join(HERE, "mix.npz"), idx=idx, **meta,
                         d_t=L("d_I.npz"), g=L("g_I.npz"), d_ee=L("d_ee_P.npz"), d_bb=L("d_bb_P.npz"),
+                        nphi_t=L("nphi_I.npz"), nphi_p=L("nphi_P.npz"),
                         mixed_grad_phi_I=sub("mixed_grad_phi_I.npz"), mixed_grad_phi_P=sub("mixed_grad_phi_P.npz"))
     for f in sorted(os.listdir(HERE)):
         if f.endswith(".npz"):
