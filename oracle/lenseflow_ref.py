@@ -903,3 +903,102 @@ def map_joint(data, noise_covariance, mixing_d, field_covariance, phi_covariance
             alpha = float(minimize(f, 1.0, method="BFGS").x[0])
         phi = phi + alpha * (hessian * grad)
     return field, phi
+
+
+# ----------------------------------------------- quadratic-estimate noise
+def _qe_k_grid(N, pix_width):
+    """simulate.py:213-228 / :254-258: KX = 2 pi fftfreq, KY = 2 pi rfftfreq (no Nyquist flip)."""
+    kx = 2 * np.pi * np.fft.fftfreq(N, pix_width)
+    ky = 2 * np.pi * np.fft.rfftfreq(N, pix_width)
+    return np.meshgrid(kx, ky, indexing="ij")
+
+
+def qe_leg(field, pix_width, encapsulated, isolated):
+    """simulate.py:272-302: (i KX)^nx (i KY)^ny F / |K|^len(isolated), NaN -> 0 (index 0 = x, 1 = y)."""
+    field = np.nan_to_num(np.asarray(field, dtype=np.complex128), nan=0)
+    idx = list(encapsulated) + list(isolated)
+    ny = sum(idx)
+    nx = len(idx) - ny
+    if nx == 0 and ny == 0:
+        return field
+    KX, KY = _qe_k_grid(field.shape[0], pix_width)
+    lap = KX ** 2 + KY ** 2
+    with np.errstate(divide="ignore", invalid="ignore"):
+        res = (1j * KX) ** nx * (1j * KY) ** ny * field / np.sqrt(lap ** len(isolated))
+    return np.nan_to_num(res, nan=0)
+
+
+def get_specific_derivative(F, pix_width, i, j):
+    """simulate.py:231-251 for two indices: d_i d_j in Fourier space (xx, yy or xy)."""
+    KX, KY = _qe_k_grid(F.shape[0], pix_width)
+    K = (KX, KY)
+    return -(K[i] * K[j]) * F
+
+
+def _indices(length):
+    """simulate.py:198-213: every 0/1 tuple of ``length``, grouped by the number of zeros."""
+    import itertools
+    out = []
+    for n0 in range(length + 1):
+        for zeros in itertools.combinations(range(length), n0):
+            p = [1] * length
+            for z in zeros:
+                p[z] = 0
+            out.append(tuple(p))
+    return out
+
+
+def scalar_quadratic_estimate(cn_tt, cf_tt, cfl_tt, m_tt, b_tt, pix_width):
+    """simulate.py:305-315 / :357-367: the T quadratic-estimate noise 1 / sum_ij |d_i d_j rfft2(internal_ij)|."""
+    N = cf_tt.shape[0]
+    irf = lambda X: np.fft.irfft2(X, s=(N, N))
+    tf = m_tt * b_tt
+    sigma = tf ** 2 * cfl_tt + cn_tt
+    with np.errstate(divide="ignore", invalid="ignore"):
+        a1, a0, a2 = tf ** 2 * cf_tt ** 2 / sigma, tf ** 2 / sigma, tf ** 2 * cf_tt / sigma
+    total = np.zeros(cf_tt.shape)
+    for i, j in _indices(2):
+        internal = (irf(qe_leg(a1, pix_width, (i, j), ())) * irf(qe_leg(a0, pix_width, (), ()))
+                    + irf(qe_leg(a2, pix_width, (i,), ())) * irf(qe_leg(a2, pix_width, (j,), ())))
+        total = total + np.abs(get_specific_derivative(np.fft.rfft2(internal), pix_width, i, j))
+    with np.errstate(divide="ignore"):
+        return np.nan_to_num(1 / total, nan=0, posinf=0, neginf=0)
+
+
+def levi_civita_3d():
+    """simulate.py:265-269."""
+    i, j, k = np.meshgrid(np.arange(3), np.arange(3), np.arange(3), indexing="ij")
+    return (i - j) * (j - k) * (k - i) / 2
+
+
+def get_polar_qe_norm_at_position(tf2e, cf_ee, sigma_e, tf2b, cf_bb, sigma_b, pix_width, i, j, k, l, m, n, p, q):
+    """simulate.py:370-385."""
+    N = cf_ee.shape[0]
+    irf = lambda X: np.fft.irfft2(X, s=(N, N))
+    with np.errstate(divide="ignore", invalid="ignore"):
+        e2, e1, e0 = tf2e * cf_ee ** 2 / sigma_e, tf2e * cf_ee / sigma_e, tf2e / sigma_e
+        b2, b1, b0 = tf2b * cf_bb ** 2 / sigma_b, tf2b * cf_bb / sigma_b, tf2b / sigma_b
+    klmn, klpq = (k, l, m, n), (k, l, p, q)
+    return (irf(qe_leg(e2, pix_width, (i, j), klmn)) * irf(qe_leg(b0, pix_width, (), klpq))
+            - 2 * irf(qe_leg(e1, pix_width, (i,), klmn)) * irf(qe_leg(b1, pix_width, (j,), klpq))
+            + irf(qe_leg(e0, pix_width, (), klmn)) * irf(qe_leg(b2, pix_width, (i, j), klpq)))
+
+
+def polar_quadratic_estimate(cf_ee, cf_bb, cfl_ee, cfl_bb, cn_ee, cn_bb, mask_ee, mask_bb, beam_ee, beam_bb,
+                             pix_width):
+    """simulate.py:318-354: the EB quadratic-estimate noise."""
+    eps = levi_civita_3d()
+    tf2e, tf2b = (mask_ee * beam_ee) ** 2, (mask_bb * beam_bb) ** 2
+    sigma_e, sigma_b = tf2e * cfl_ee + cn_ee, tf2b * cfl_bb + cn_bb
+    total = np.zeros(cf_ee.shape)
+    for i, j in _indices(2):
+        internal = np.zeros((cf_ee.shape[0],) * 2)
+        for (k, l, m, n, p, q) in _indices(6):
+            w = 4 * eps[m, p, 2] * eps[n, q, 2]
+            if w == 0:
+                continue
+            internal = internal + w * get_polar_qe_norm_at_position(tf2e, cf_ee, sigma_e, tf2b, cf_bb, sigma_b,
+                                                                    pix_width, i, j, k, l, m, n, p, q)
+        total = total + np.abs(get_specific_derivative(np.fft.rfft2(internal), pix_width, i, j))
+    with np.errstate(divide="ignore"):
+        return np.nan_to_num(1 / total, nan=0, posinf=0, neginf=0)

@@ -174,3 +174,29 @@ def test_unmix_inverts_mix():
     for nm in ("polar_matrix_1", "polar_matrix_2"):
         a, b = getattr(f, nm)[:, 1:-1], getattr(S["field"], nm)[:, 1:-1]
         assert rel_l2(a, b) < 1e-4
+
+
+@pytest.mark.parametrize("which", ["I", "P"])
+def test_quadratic_estimate_near_julia(which):
+    """simulate.py:305-354 against Julia's N_phi: an approximate pin only.
+
+    The reference divides its estimate by nphi_fac = 2 (simulate.py:638,
+    :716-720) and feeds CAMB's lensed spectra, which the fixtures lack; with
+    the unlensed spectrum in their place the median ratio to Julia's N_phi is
+    1.82 (T) / 1.95 (QU), so the estimate / 2 sits within 10% of Julia's on
+    half of the modes.
+    """
+    pw = R.pix_width_of(2.5)
+    m = load_golden("mix.npz")
+    if which == "I":
+        g = load_golden("infer_I.npz")
+        qe = R.scalar_quadratic_estimate(g["cn"], g["cf"], g["cf"], g["m"], g["b"], pw)
+        nphi = m["nphi_t"]
+    else:
+        g = load_golden("infer_P.npz")
+        qe = R.polar_quadratic_estimate(g["cf_ee"], g["cf_bb"], g["cf_ee"], g["cf_bb"], g["cn_ee"], g["cn_bb"],
+                                        g["m_ee"], g["m_bb"], g["b_ee"], g["b_bb"], pw)
+        nphi = m["nphi_p"]
+    sel = (qe != 0) & (nphi != 0)
+    ratio = np.median(np.real(qe[sel]) / np.real(nphi[sel])) / 2
+    assert 0.85 < ratio < 1.05, ratio
