@@ -227,15 +227,19 @@ class HostPipeline:
     Each call copies f [B,C,N,N] and phi [B,N,N] (pinned host memory) to the
     device, computes the phi derivative planes (with the magnification check),
     lenses, and copies the result back into a pinned host buffer.  The batch
-    is split into ``chunks``: the host-to-device copy of chunk i+1, the compute
-    of chunk i and the device-to-host copy of chunk i-1 run on three streams
-    at once, with double-buffered device slots.  The magnification minima are
-    read back once per call, after the last chunk; a call whose phi is
-    singular raises SingularMagnificationError (its outputs are then
-    meaningless).  Device buffers are allocated once.
+    is split into ``chunks`` that move through ``slots`` sets of device
+    buffers: host-to-device copies on one stream, compute alternating between
+    ``compute_streams`` streams, device-to-host copies on another.  A chunk's
+    lens is a few dozen short launches; with two compute streams the kernels
+    of neighbouring chunks fill each other's tail waves and launch gaps, so
+    smaller chunks (better copy overlap) stop costing compute throughput.
+    The magnification minima are read back once per call, after the last
+    chunk; a call whose phi is singular raises SingularMagnificationError (its
+    outputs are then meaningless).  Device buffers are allocated once (the
+    lens workspace at the first call, when n is known).
     """
 
-    def __init__(self, plan, batch, io_dtype=torch.float64, chunks=4):
+    def __init__(self, plan, batch, io_dtype=torch.float64, chunks=16, compute_streams=2, slots=4):
         self.plan = plan
         N, C = plan.nside, plan.ncomp
         dev = plan.device
@@ -244,15 +248,18 @@ class HostPipeline:
         self.cb = -(-batch // self.chunks)  # maps per chunk (last may be shorter)
         cb = self.cb
         self.io_dtype = io_dtype
-        self.d_f = [torch.empty((cb, C, N, N), dtype=io_dtype, device=dev) for _ in range(2)]
-        self.d_out = [torch.empty((cb, C, N, N), dtype=io_dtype, device=dev) for _ in range(2)]
-        self.d_phi = [torch.empty((cb, N, N), dtype=torch.float64, device=dev) for _ in range(2)]
-        self.planes = torch.empty((cb, 5, N, N), dtype=plan.dtype, device=dev)
-        self.ws = torch.empty(16, dtype=torch.uint8, device=dev)  # sized for n at the first call
-        self.phi_ws = torch.empty(max(plan.phi_workspace_bytes(cb), 16), dtype=torch.uint8, device=dev)
+        self.nslots = max(2, int(slots))
+        ns = self.nslots
+        self.d_f = [torch.empty((cb, C, N, N), dtype=io_dtype, device=dev) for _ in range(ns)]
+        self.d_out = [torch.empty((cb, C, N, N), dtype=io_dtype, device=dev) for _ in range(ns)]
+        self.d_phi = [torch.empty((cb, N, N), dtype=torch.float64, device=dev) for _ in range(ns)]
+        self.planes = [torch.empty((cb, 5, N, N), dtype=plan.dtype, device=dev) for _ in range(ns)]
+        self.ws = [torch.empty(16, dtype=torch.uint8, device=dev) for _ in range(ns)]  # sized for n at first call
+        self.phi_ws = [torch.empty(max(plan.phi_workspace_bytes(cb), 16), dtype=torch.uint8, device=dev)
+                       for _ in range(ns)]
         self.min_det = torch.empty(max(self.chunks * cb, 1), dtype=torch.int32, device=dev)
         self.s_in = torch.cuda.Stream(dev)
-        self.s_cmp = torch.cuda.Stream(dev)
+        self.s_cmp = [torch.cuda.Stream(dev) for _ in range(max(1, int(compute_streams)))]
         self.s_out = torch.cuda.Stream(dev)
 
     def h2d_bytes(self):
@@ -266,50 +273,56 @@ class HostPipeline:
     def __call__(self, f_host, phi_host, out_host, n=10, direction=FORWARD_LENSE, adjoint=False, check_det=True):
         plan, lib = self.plan, self.plan._lib
         need = plan.workspace_bytes(self.cb, True, n)
-        if self.ws.numel() < need:
-            self.ws = torch.empty(need, dtype=torch.uint8, device=plan.device)
+        for k in range(self.nslots):
+            if self.ws[k].numel() < need:
+                self.ws[k] = torch.empty(need, dtype=torch.uint8, device=plan.device)
         cur = torch.cuda.current_stream(plan.device)
-        for st in (self.s_in, self.s_cmp, self.s_out):
+        streams = [self.s_in, self.s_out] + self.s_cmp
+        for st in streams:
             st.wait_stream(cur)
+        first = self.s_cmp[0]
         if check_det:
-            with torch.cuda.stream(self.s_cmp):
+            with torch.cuda.stream(first):
                 nat.check(lib.lf_min_det_init(_ptr(self.min_det), self.min_det.numel(), _stream_ptr(plan.device)),
                           "lf_min_det_init")
+            for st in self.s_cmp[1:]:
+                st.wait_stream(first)
         ev_in = [torch.cuda.Event() for _ in range(self.chunks)]
         ev_cmp = [torch.cuda.Event() for _ in range(self.chunks)]
         ev_out = [torch.cuda.Event() for _ in range(self.chunks)]
-        N, C = plan.nside, plan.ncomp
+        ns = self.nslots
         for i in range(self.chunks):
             lo, hi = i * self.cb, min((i + 1) * self.cb, self.batch)
             m = hi - lo
             if m <= 0:
                 break
-            slot = i % 2
+            slot = i % ns
             with torch.cuda.stream(self.s_in):
-                if i >= 2:
-                    self.s_in.wait_event(ev_cmp[i - 2])  # the slot's previous chunk has been consumed
+                if i >= ns:
+                    self.s_in.wait_event(ev_cmp[i - ns])  # the slot's previous chunk has been consumed
                 self.d_f[slot][:m].copy_(f_host[lo:hi], non_blocking=True)
                 self.d_phi[slot][:m].copy_(phi_host[lo:hi], non_blocking=True)
                 ev_in[i].record(self.s_in)
-            with torch.cuda.stream(self.s_cmp):
-                self.s_cmp.wait_event(ev_in[i])
-                if i >= 2:
-                    self.s_cmp.wait_event(ev_out[i - 2])  # the slot's previous output has been copied out
+            sc = self.s_cmp[i % len(self.s_cmp)]
+            with torch.cuda.stream(sc):
+                sc.wait_event(ev_in[i])
+                if i >= ns:
+                    sc.wait_event(ev_out[i - ns])  # the slot's previous output has been copied out
                 st = _stream_ptr(plan.device)
                 md = _ptr(self.min_det[lo:]) if check_det else None
                 nat.check(lib.lf_phi_precompute(plan.handle, _ptr(self.d_phi[slot]), nat.LF_PHI_MAP, m,
-                                                _ptr(self.planes), md, _ptr(self.phi_ws), self.phi_ws.numel(), st),
-                          "lf_phi_precompute")
+                                                _ptr(self.planes[slot]), md, _ptr(self.phi_ws[slot]),
+                                                self.phi_ws[slot].numel(), st), "lf_phi_precompute")
                 code = nat.LF_F64 if self.io_dtype == torch.float64 else nat.LF_F32
                 nat.check(lib.lf_lense_flow(plan.handle, _ptr(self.d_f[slot]), code, _ptr(self.d_out[slot]), code,
-                                            _ptr(self.planes), m, int(n), int(direction), int(bool(adjoint)),
-                                            _ptr(self.ws), self.ws.numel(), st), "lf_lense_flow")
-                ev_cmp[i].record(self.s_cmp)
+                                            _ptr(self.planes[slot]), m, int(n), int(direction), int(bool(adjoint)),
+                                            _ptr(self.ws[slot]), self.ws[slot].numel(), st), "lf_lense_flow")
+                ev_cmp[i].record(sc)
             with torch.cuda.stream(self.s_out):
                 self.s_out.wait_event(ev_cmp[i])
                 out_host[lo:hi].copy_(self.d_out[slot][:m], non_blocking=True)
                 ev_out[i].record(self.s_out)
-        for st in (self.s_in, self.s_cmp, self.s_out):
+        for st in streams:
             cur.wait_stream(st)
         if check_det:
             vals = [lib.lf_decode_min_det(int(v)) for v in self.min_det[:self.batch].cpu().tolist()]
