@@ -589,6 +589,175 @@ __global__ void __launch_bounds__(NT, MINB) k_row_pair(StageArgs a) {
   }
 }
 
+// ==================================== adjoint row pass, component pairs
+// The adjoint RHS k_c = d_x(p_x y_c) + d_y(p_y y_c) for two components with
+// the p planes, N = 512, FP32.  Each component's rate spectrum
+// K_c = Gx_c + i KY V_c / N is Hermitian, so both rates come from one
+// full-length inverse FFT of Z = K_0 + i K_1 (z = k_0 + i k_1).  After the
+// RK4 update the next stage's four real inputs pair up as
+// w_u = p_x y_0 + i p_x y_1 and w_v = p_y y_0 + i p_y y_1 (p at the next
+// stage time): two forward FFTs, split into the packed spectra U_c (a.s) and
+// V_c (a.v) as in k_row_pair.  Same staging, passes and bounded wait.
+template <int N, int LINES, int NT, int MINB>
+__global__ void __launch_bounds__(NT, MINB) k_row_pair_adj(StageArgs a) {
+  using T = float;
+  constexpr int H = N / 2;
+  constexpr long P = (long)N * N;
+  constexpr int R = 8, NB = N / R;
+  static_assert(N == 512, "three radix-8 passes");
+  static_assert(NB * LINES == NT, "one (row, butterfly) per thread in the fused passes");
+  constexpr int TILE = LINES * N;
+  constexpr int RB = LINES * N;
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  c2<T>* tw = reinterpret_cast<c2<T>*>(smem_raw);
+  c2<T>* buf = tw + N;                            // Z (tile 0); then w_u (tile 0), w_v (tile 1)
+  T* stg = reinterpret_cast<T*>(buf + 2 * TILE);  // y0_0, y0_1, acc_0, acc_1, p_x, p_y
+  uint64_t* mbar = reinterpret_cast<uint64_t*>(stg + 6 * RB);
+  const int tid = threadIdx.x;
+  const int r0 = blockIdx.x * LINES;
+  const long map = blockIdx.y;
+  const long prow0 = (long)r0 * N;
+  const bool with_acc = a.stage > 1;
+  if (tid == 0) {
+    mbar_init(mbar, 1);
+    mbar_expect_tx(mbar, uint32_t((with_acc ? 6 : 4) * RB * sizeof(T)));
+    const T* pp = reinterpret_cast<const T*>(a.pp) + (map * a.pp_k + a.pp_idx) * 2 * P + prow0;
+    for (int c = 0; c < 2; ++c) {
+      bulk_g2s(stg + c * RB, reinterpret_cast<const T*>(a.y0) + (map * 2 + c) * P + prow0, RB * sizeof(T), mbar);
+      if (with_acc)
+        bulk_g2s(stg + (2 + c) * RB, reinterpret_cast<const T*>(a.acc) + (map * 2 + c) * P + prow0, RB * sizeof(T),
+                 mbar);
+      bulk_g2s(stg + (4 + c) * RB, pp + c * P, RB * sizeof(T), mbar);
+    }
+  }
+  load_twiddles<T, ptw_size(N), NT>(tw, a.twP, tid);
+  constexpr int O8 = ptw_offset(N, R, R), O64 = ptw_offset(N, R, R * R);
+  const T ky_scale = T(a.kbase / double(N));
+  const long half_plane = N * (long)H;
+  auto spec = [&](void* base, int c) {
+    return reinterpret_cast<c2<T>*>(base) + (map * 2 + c) * half_plane + (long)r0 * H;
+  };
+
+  // -------------------- load: Z = K_0 + i K_1, K_c = Gx_c + i KY V_c / N (Hermitian)
+#pragma unroll
+  for (int idx = tid; idx < LINES * (H / 2); idx += NT) {
+    const int t = idx % (H / 2), row = idx / (H / 2);
+    c2<T> g0[2], g1[2], v0[2], v1[2];
+    ld2<T>(spec(a.gx, 0) + row * H + 2 * t, g0);
+    ld2<T>(spec(a.gx, 1) + row * H + 2 * t, g1);
+    ld2<T>(spec(a.v, 0) + row * H + 2 * t, v0);
+    ld2<T>(spec(a.v, 1) + row * H + 2 * t, v1);
+#pragma unroll
+    for (int q = 0; q < 2; ++q) {
+      const int k = 2 * t + q;
+      if (k == 0) {  // real DC and Nyquist bins of each rate; i KY contributes nothing there
+        buf[sw<T, LINES>(0, row)] = mk<T>(g0[0].x, g1[0].x);
+        buf[sw<T, LINES>(H, row)] = mk<T>(g0[0].y, g1[0].y);
+      } else {
+        const T f = ky_scale * T(k);
+        const c2<T> k0 = mk<T>(g0[q].x - f * v0[q].y, g0[q].y + f * v0[q].x);  // Gx + i f V
+        const c2<T> k1 = mk<T>(g1[q].x - f * v1[q].y, g1[q].y + f * v1[q].x);
+        buf[sw<T, LINES>(k, row)] = mk<T>(k0.x - k1.y, k0.y + k1.x);            // K_0 + i K_1
+        buf[sw<T, LINES>(N - k, row)] = mk<T>(k0.x + k1.y, k1.x - k0.y);        // conj(K_0) + i conj(K_1)
+      }
+    }
+  }
+  __syncthreads();
+  stockham_pass<T, N, R, 1, LINES, 1, NT, true, N, true>(buf, tw, tid);
+  stockham_pass<T, N, R, R, LINES, 1, NT, true, N, true>(buf, tw + O8, tid);
+
+  // ------------- inverse pass 3 -> RK4 update -> two forward first passes, in registers
+  const int j = tid % NB, row = tid / NB;
+  c2<T> z[R];
+#pragma unroll
+  for (int r = 0; r < R; ++r) z[r] = buf[sw<T, LINES>(j + r * NB, row)];
+#pragma unroll
+  for (int r = 1; r < R; ++r) z[r] = twmul<T, true>(z[r], tw[O64 + (r - 1) * NB + j]);
+  dft<R, T, true>(z);
+  // z[r] = (k_0, k_1) at pixel n = j + NB r of row r0 + row
+  if (!mbar_wait(mbar, 0, kWaitTries)) {
+    atomicExch(&g_lf_wait_timeouts, 1);
+    mbar_wait(mbar, 0, kWaitTries);
+    return;
+  }
+  const long prow = prow0 + (long)row * N;
+  const T* sy0 = stg + row * N;
+  const T* sacc = stg + 2 * RB + row * N;
+  const T* spx = stg + 4 * RB + row * N;
+  const T* spy = stg + 5 * RB + row * N;
+  const T hh = T(a.h);
+  c2<T> wu[R], wv[R];
+#pragma unroll
+  for (int r = 0; r < R; ++r) {
+    const int n = j + NB * r;
+    T yn[2];
+#pragma unroll
+    for (int c = 0; c < 2; ++c) {
+      const T k = c == 0 ? z[r].x : z[r].y;
+      const T y0 = sy0[c * RB + n];
+      T* accg = reinterpret_cast<T*>(a.acc) + (map * 2 + c) * P + prow;
+      if (a.stage == 1) {
+        yn[c] = y0 + T(0.5) * hh * k;
+        accg[n] = k;
+      } else if (a.stage < 4) {
+        yn[c] = y0 + (a.stage == 2 ? T(0.5) * hh : hh) * k;
+        accg[n] = sacc[c * RB + n] + T(2) * k;
+      } else {
+        yn[c] = y0 + hh / T(6) * (sacc[c * RB + n] + k);
+        if (a.last) {
+          const long fo = (map * 2 + c) * P + prow + n;
+          if (a.out_f64) reinterpret_cast<double*>(a.f_out)[fo] = double(yn[c]);
+          else reinterpret_cast<float*>(a.f_out)[fo] = yn[c];
+        } else {
+          reinterpret_cast<T*>(a.y0)[(map * 2 + c) * P + prow + n] = yn[c];
+        }
+      }
+    }
+    const T px = spx[n], py = spy[n];  // p at the next stage's time
+    wu[r] = mk<T>(px * yn[0], px * yn[1]);
+    wv[r] = mk<T>(py * yn[0], py * yn[1]);
+  }
+  if (a.last) return;  // uniform across the block
+  dft<R, T, false>(wu);  // forward pass 1 (NS = 1) of both: outputs at 8 j + r
+  dft<R, T, false>(wv);
+  __syncthreads();       // every thread has read its inverse-pass-3 inputs
+#pragma unroll
+  for (int r = 0; r < R; ++r) {
+    buf[sw<T, LINES>(R * j + r, row)] = wu[r];
+    buf[TILE + sw<T, LINES>(R * j + r, row)] = wv[r];
+  }
+  __syncthreads();
+  stockham_pass<T, N, R, R, LINES, 2, NT, false, N, true>(buf, tw + O8, tid);
+  stockham_pass<T, N, R, R * R, LINES, 2, NT, false, N, true>(buf, tw + O64, tid);
+
+  // ----------------- split W_u into U_0, U_1 (a.s) and W_v into V_0, V_1 (a.v)
+#pragma unroll
+  for (int idx = tid; idx < 2 * LINES * (H / 2); idx += NT) {
+    const int t = idx % (H / 2), rest = idx / (H / 2);
+    const int rw = rest % LINES, which = rest / LINES;
+    const c2<T>* wb = buf + which * TILE;
+    c2<T> s0[2], s1[2];
+#pragma unroll
+    for (int q = 0; q < 2; ++q) {
+      const int k = 2 * t + q;
+      if (k == 0) {
+        const c2<T> w0 = wb[sw<T, LINES>(0, rw)], wh = wb[sw<T, LINES>(H, rw)];
+        s0[0] = mk<T>(w0.x, wh.x);
+        s1[0] = mk<T>(w0.y, wh.y);
+      } else {
+        const c2<T> A = wb[sw<T, LINES>(k, rw)];
+        const c2<T> B = cconj<T>(wb[sw<T, LINES>(N - k, rw)]);
+        s0[q] = cscale<T>(cadd<T>(A, B), T(0.5));
+        const c2<T> d = csub<T>(A, B);
+        s1[q] = mk<T>(T(0.5) * d.y, T(-0.5) * d.x);  // (A - B) / 2i
+      }
+    }
+    void* dst = which == 0 ? a.s : a.v;
+    st2<T>(spec(dst, 0) + rw * H + 2 * t, s0);
+    st2<T>(spec(dst, 1) + rw * H + 2 * t, s1);
+  }
+}
+
 // ====================================================== p planes
 // p = M(t)^-1 grad(phi), M = I + t grad grad phi (lense_flow.py:373-381,
 // :398-415), at the K = 2n+1 stage times t_k = t0 + k hh of an RK4

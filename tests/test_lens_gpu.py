@@ -46,8 +46,8 @@ def _engine(torch, f, phis, pw, n, direction, adjoint, precision="f32"):
                                        (512, 2.0, 2)])
 @pytest.mark.parametrize("direction,adjoint", [(1, False), (-1, False), (1, True), (-1, True)])
 def test_lens_matches_oracle(torch_cuda, N, theta, C, direction, adjoint):
-    if N == 512 and (direction, adjoint) != (1, False):
-        pytest.skip("512^2 covered for the forward lens; the other modes are covered at smaller N")
+    if N == 512 and (direction, adjoint) == (-1, False):
+        pytest.skip("512^2 inverse lens runs the forward kernels with direction -1; covered at smaller N")
     f, phis = _inputs(N, theta, C)
     pw = R.pix_width_of(theta)
     got = _engine(torch_cuda, f, phis, pw, 7, direction, adjoint)[0]
@@ -85,14 +85,16 @@ def test_p_plane_and_derivative_plane_paths(torch_cuda, C, direction, adjoint):
 
 
 def test_qu512_stage_waits_complete(torch_cuda):
-    """The 512^2 QU stage kernel stages its operands with bulk copies; every block's bounded wait completes."""
+    """The 512^2 QU stage kernels (standard and adjoint) stage their operands with bulk copies; every block's
+    bounded wait completes."""
     import torch
     from cmblensing_b200 import engine
     engine.wait_timeouts(reset=True)
     f, phis = _inputs(512, 2.0, 2, B=3, seed0=9)
     pw = R.pix_width_of(2.0)
     for direction in (1, -1):
-        _engine(torch, f, phis, pw, 7, direction, False)
+        for adjoint in (False, True):
+            _engine(torch, f, phis, pw, 7, direction, adjoint)
     torch.cuda.synchronize()
     assert engine.wait_timeouts() == 0
 
@@ -192,6 +194,33 @@ def test_round_trip_512_QU(torch_cuda):
         den += float(np.sum(f[b] ** 2))
     ref = np.sqrt(num / den)
     assert abs(err - ref) / ref < 1e-2, (err, ref)
+
+
+def test_qu512_paired_adjoint(torch_cuda):
+    """The 512^2 QU adjoint with p planes (one paired transform for both rates) matches the five-plane adjoint,
+    and <L a, L a> == <a, L^T L a> to FP32 rounding."""
+    import torch
+    from cmblensing_b200 import engine
+    N, theta, n, B = 512, 2.0, 7, 2
+    f, phis = _inputs(N, theta, 2, B=B, seed0=21)
+    pw = R.pix_width_of(theta)
+    plan = engine.get_plan(N, 2, pw)
+    planes = plan.phi_planes(torch.as_tensor(phis, device="cuda"))
+    a = torch.as_tensor(f, device="cuda", dtype=torch.float32)
+    rng = np.random.default_rng(4)
+    b = torch.as_tensor(rng.standard_normal(f.shape), device="cuda", dtype=torch.float32)
+    outs = []
+    for nbytes in (plan.workspace_bytes(B, True), plan.workspace_bytes(B, True, n)):
+        ws = torch.empty(nbytes, dtype=torch.uint8, device="cuda")
+        outs.append(plan.lense_flow(b, planes, n=n, adjoint=True, workspace=ws).double())
+    assert float(torch.linalg.vector_norm(outs[0] - outs[1]) / torch.linalg.vector_norm(outs[0])) < 1e-6
+    # <L a, L a> == <a, L^T (L a)>: positive on both sides, so FP32 rounding is not amplified by cancellation
+    La = plan.lense_flow(a, planes, n=n)
+    LTLa = plan.lense_flow(La, planes, n=n, adjoint=True).double()
+    for m in range(B):
+        lhs = float((La[m].double() ** 2).sum())
+        rhs = float((a[m].double() * LTLa[m]).sum())
+        assert abs(lhs - rhs) / abs(lhs) < 1e-5, (m, lhs, rhs)
 
 
 def test_adjoint_dot_product(torch_cuda):
