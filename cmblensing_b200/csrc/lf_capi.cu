@@ -40,7 +40,10 @@ struct lf_plan_s {
   int device;
   void* tw;        // N complex values in the compute precision
   double2* tw64;   // N complex float64 (phi precompute)
-  void* twp;       // pass table of length N in the compute precision
+  void* twp;       // pass table of length N, then the column table, in the compute precision
+  const void* twc() const {  // the column table inside twp
+    return static_cast<const char*>(twp) + (prec == LF_F64 ? sizeof(double2) : sizeof(float2)) * ptw_size(N);
+  }
 };
 
 // Pass table of length L (layout: ptw_offset / ptw_size): store(i, cos, sin)
@@ -55,6 +58,23 @@ static void fill_pass_table(int L, Store store) {
       for (int k = 0; k < x.NS; ++k) {
         const double ang = -2.0 * M_PI * (double)r * (double)k / ((double)x.R * (double)x.NS);
         store(off + (r - 1) * x.NS + k, std::cos(ang), std::sin(ang));
+      }
+  }
+}
+
+// Column table of the two-pass column plan (layout: ctw_inv_offset /
+// ctw_size): the forward pass-2 block (R2 after R1), then the inverse pass-2
+// block (R1 after R2); W^{r k} at (r - 1) NS + k of each, float64 values.
+template <class Store>
+static void fill_col_table(int L, Store store) {
+  if (!col2_plan(L)) return;
+  const int blocks[2][3] = {{col2_r2(L), col2_r1(L), 0}, {col2_r1(L), col2_r2(L), ctw_inv_offset(L)}};
+  for (const auto& b : blocks) {
+    const int R = b[0], NS = b[1], off = b[2];
+    for (int r = 1; r < R; ++r)
+      for (int k = 0; k < NS; ++k) {
+        const double ang = -2.0 * M_PI * (double)r * (double)k / ((double)R * (double)NS);
+        store(off + (r - 1) * NS + k, std::cos(ang), std::sin(ang));
       }
   }
 }
@@ -132,19 +152,31 @@ cudaError_t launch(dim3 grid, int nt, size_t smem, cudaStream_t st, Args... args
   return launch_k<Kernel>(LF_KIND_PHI, grid, nt, smem, st, args...);
 }
 
+// One column pass over `planes` packed row-spectrum planes.  FP32 512: the
+// two-pass plan 16 x 32 in 256-thread blocks; otherwise the pass-table plan.
+template <typename T, int N>
+cudaError_t launch_col(int planes, cudaStream_t st, const StageArgs& a) {
+  constexpr int LINES = Geo<T>::LINES;
+  const dim3 grid(N / 2 / LINES, planes);
+  if constexpr (std::is_same<T, float>::value && col2_plan(N)) {
+    constexpr int NT2 = 256;
+    const size_t smem = sizeof(c2<T>) * (col_tw_entries(N, true) + LINES * N);
+    return launch_k<k_col<T, N, LINES, NT2, 2, true>>(LF_KIND_COL, grid, NT2, smem, st, a);
+  } else {
+    constexpr int NT = Geo<T>::nt(N);
+    const size_t smem = sizeof(c2<T>) * (col_tw_entries(N) + LINES * N);
+    return launch_k<k_col<T, N, LINES, NT, Geo<T>::minb(N)>>(LF_KIND_COL, grid, NT, smem, st, a);
+  }
+}
+
 template <typename T, int N, int C, bool ADJ, bool PP>
 cudaError_t run_lens_pp(const StageArgs& base, int B, int nsteps, double t0, double t1, cudaStream_t st) {
-  constexpr int LINES = Geo<T>::LINES;
   constexpr int RL = Geo<T>::ROW_LINES;
-  constexpr int NT = Geo<T>::nt(N);
-  constexpr int MB = Geo<T>::minb(N);
   constexpr int RNT = Geo<T>::row_nt(N);
   constexpr int RMB = Geo<T>::row_minb(N);
   constexpr int H = N / 2;
   const size_t smem_row = sizeof(c2<T>) * (N + 2 * C * RL * H);
-  const size_t smem_col = sizeof(c2<T>) * (col_tw_entries(N) + LINES * N);
   const dim3 grow(N / RL, B);
-  const dim3 gcol(H / LINES, B * C);
   StageArgs a = base;
   cudaError_t e;
   const double h = (t1 - t0) / nsteps;  // util.py:185
@@ -179,7 +211,7 @@ cudaError_t run_lens_pp(const StageArgs& base, int B, int nsteps, double t0, dou
       a.t_next = tn[s];
       a.pp_idx = ADJ ? kn[s] : kc[s];
       a.last = (i == nsteps - 1 && s == 3);
-      e = launch_k<k_col<T, N, LINES, NT, MB>>(LF_KIND_COL, gcol, NT, smem_col, st, a);
+      e = launch_col<T, N>(B * C, st, a);
       if (e != cudaSuccess) return e;
       if constexpr (PP && C == 2 && !ADJ && N == 512 && std::is_same<T, float>::value) {
         // two components: full-length complex transforms, update fused in registers;
@@ -358,17 +390,12 @@ struct VjpLayout {
 template <typename T, int N, int C>
 cudaError_t run_vjp_n(const StageArgs& af0, const StageArgs& ad0, double* dacc, int B, int nsteps, double t0,
                       double t1, cudaStream_t st) {
-  constexpr int LINES = Geo<T>::LINES;
   constexpr int RL = Geo<T>::ROW_LINES;
-  constexpr int NT = Geo<T>::nt(N);
-  constexpr int MB = Geo<T>::minb(N);
   constexpr int RNT = Geo<T>::row_nt(N);
   constexpr int RMB = Geo<T>::row_minb(N);
   constexpr int H = N / 2;
   const size_t smem_row = sizeof(c2<T>) * (N + 2 * C * RL * H);
-  const size_t smem_col = sizeof(c2<T>) * (col_tw_entries(N) + LINES * N);
   const dim3 grow(N / RL, B);
-  const dim3 gcol(H / LINES, B * C);
   const long P = (long)N * N;
   const int gacc = (int)std::min<long>(((long)B * P + 255) / 256, 4096);
   StageArgs af = af0, ad = ad0;
@@ -393,14 +420,14 @@ cudaError_t run_vjp_n(const StageArgs& af0, const StageArgs& ad0, double* dacc, 
       af.t_cur = ad.t_cur = tc[s];
       af.t_next = ad.t_next = tn[s];
       af.last = ad.last = last;
-      e = launch_k<k_col<T, N, LINES, NT, MB>>(LF_KIND_COL, gcol, NT, smem_col, st, af);
+      e = launch_col<T, N>(B * C, st, af);
       if (e != cudaSuccess) return e;
       e = launch_k<k_row<T, N, C, false, false, RL, RNT, true, RMB>>(LF_KIND_ROW, grow, RNT, smem_row, st, af);
       if (e != cudaSuccess) return e;
       e = launch<k_dphi_accum<T, C>>(dim3(gacc), 256, 0, st, (const T*)af.grad, (const T*)ad.dsave,
                                      (const T*)af.phi, dacc, B, P, tc[s], h / 6.0 * cw[s], (int)(i == 0 && s == 0));
       if (e != cudaSuccess) return e;
-      e = launch_k<k_col<T, N, LINES, NT, MB>>(LF_KIND_COL, gcol, NT, smem_col, st, ad);
+      e = launch_col<T, N>(B * C, st, ad);
       if (e != cudaSuccess) return e;
       e = launch_k<k_row<T, N, C, true, false, RL, RNT, true, RMB>>(LF_KIND_ROW, grow, RNT, smem_row, st, ad);
       if (e != cudaSuccess) return e;
@@ -484,13 +511,15 @@ int lf_plan_create(lf_plan_t* out, int nside, int ncomp, double pix_width, int p
     }
   }
   if (e == cudaSuccess) {
-    const size_t np = (size_t)ptw_size(nside);
+    const size_t np = (size_t)ptw_size(nside) + (size_t)ctw_size(nside);
     std::vector<double2> pt(np);
     std::vector<float2> pt32(np);
-    fill_pass_table(nside, [&](int i, double c, double sn) {
+    auto put = [&](int i, double c, double sn) {
       pt[i] = make_double2(c, sn);
       pt32[i] = make_float2((float)c, (float)sn);
-    });
+    };
+    fill_pass_table(nside, put);
+    fill_col_table(nside, [&](int i, double c, double sn) { put(ptw_size(nside) + i, c, sn); });
     const bool f64 = precision == LF_F64;
     const size_t bytes = f64 ? sizeof(double2) * np : sizeof(float2) * np;
     e = cudaMalloc(&p->twp, bytes);
@@ -619,6 +648,7 @@ int lf_lense_flow(lf_plan_t p, const void* f_in, int in_dtype, void* f_out, int 
   if (ppb && ws_bytes >= base_bytes + ppb) a.pp = w + base_bytes;
   a.twN = p->tw;
   a.twP = p->twp;
+  a.twC = p->twc();
   a.kbase = 2.0 * M_PI / ((double)p->N * p->pix_width);
   a.nplanes = batch * p->C;
   cudaError_t e;
@@ -716,6 +746,7 @@ int lf_lense_flow_vjp(lf_plan_t p, const void* f_lensed, const void* cotangent, 
   af.gx = fs + 3 * plane;
   af.twN = p->tw;
   af.twP = p->twp;
+  af.twC = p->twc();
   af.kbase = 2.0 * M_PI / ((double)p->N * p->pix_width);
   af.nplanes = batch * p->C;
   af.grad = grad;
@@ -792,8 +823,9 @@ int lf_profile_read(lf_plan_t p, int kind, double* total_ms, int* launches) {
 // on the first call on the device, and only those addresses reach kernels.
 static __device__ __align__(256) unsigned char g_noalloc_scratch[LF_NOALLOC_SCRATCH_BYTES];
 static __device__ __align__(256) float2 g_noalloc_tw[64 + 128 + 256 + 512 + 1024];
-// pass tables (column pass) of every supported N, back to back
-constexpr int kNoAllocTwp = ptw_size(64) + ptw_size(128) + ptw_size(256) + ptw_size(512) + ptw_size(1024);
+// pass table + column table of every supported N, back to back
+constexpr int twp_entries(int n) { return ptw_size(n) + ctw_size(n); }
+constexpr int kNoAllocTwp = twp_entries(64) + twp_entries(128) + twp_entries(256) + twp_entries(512) + twp_entries(1024);
 static __device__ __align__(256) float2 g_noalloc_twp[kNoAllocTwp];
 
 namespace {
@@ -815,7 +847,7 @@ int noalloc_tw_offset(int n) {
 
 int noalloc_twp_offset(int n) {
   int off = 0;
-  for (int m = 64; m < n; m *= 2) off += ptw_size(m);
+  for (int m = 64; m < n; m *= 2) off += twp_entries(m);
   return off;
 }
 
@@ -853,6 +885,9 @@ int noalloc_setup(NoAllocDevice** out) {
     for (int n = 64; n <= 1024; n *= 2) {
       const int off = noalloc_twp_offset(n);
       fill_pass_table(n, [&](int i, double c, double sn) { host_p[off + i] = make_float2((float)c, (float)sn); });
+      fill_col_table(n, [&](int i, double c, double sn) {
+        host_p[off + ptw_size(n) + i] = make_float2((float)c, (float)sn);
+      });
     }
     e = cudaMemcpyToSymbol(g_noalloc_twp, host_p, sizeof(host_p));
     if (e != cudaSuccess) return cuda_status(e);
@@ -906,6 +941,7 @@ extern "C" int lf_lense_flow_noalloc(int nside, int ncomp, double pix_width, con
   a.v = adj ? (void*)(d->scratch + 4 * plane_bytes) : nullptr;
   a.twN = d->tw + noalloc_tw_offset(nside);
   a.twP = d->twp + noalloc_twp_offset(nside);
+  a.twC = d->twp + noalloc_twp_offset(nside) + ptw_size(nside);
   a.kbase = 2.0 * M_PI / ((double)nside * pix_width);
   a.nplanes = batch * ncomp;
   g_prof = nullptr;

@@ -129,12 +129,43 @@ template <typename T, bool INV> __device__ __forceinline__ void dft16(c2<T>* a) 
   }
 }
 
+// cos(pi/16), sin(pi/16), cos(3 pi/16), sin(3 pi/16)
+#define LF_C11 0.98078528040323044913
+#define LF_S11 0.19509032201612826785
+#define LF_C33 0.83146961230254523708
+#define LF_S33 0.55557023301960222474
+
+// Radix-2 split into two 16-point DFTs: X[k] = E[k] + W32^k O[k], X[k+16] = E[k] - W32^k O[k].
+template <typename T, bool INV> __device__ __forceinline__ void dft32(c2<T>* a) {
+  c2<T> e[16], o[16];
+#pragma unroll
+  for (int i = 0; i < 16; ++i) {
+    e[i] = a[2 * i];
+    o[i] = a[2 * i + 1];
+  }
+  dft16<T, INV>(e);
+  dft16<T, INV>(o);
+  // W32^k forward = (cos(pi k/16), -sin(pi k/16)), k = 0..15
+  const T wr[16] = {T(1),       T(LF_C11),  T(LF_C22),  T(LF_C33),  T(LF_C45), T(LF_S33),  T(LF_S22),  T(LF_S11),
+                    T(0),       T(-LF_S11), T(-LF_S22), T(-LF_S33), T(-LF_C45), T(-LF_C33), T(-LF_C22), T(-LF_C11)};
+  const T ws[16] = {T(0),      T(LF_S11), T(LF_S22), T(LF_S33), T(LF_C45), T(LF_C33), T(LF_C22), T(LF_C11),
+                    T(1),      T(LF_C11), T(LF_C22), T(LF_C33), T(LF_C45), T(LF_S33), T(LF_S22), T(LF_S11)};
+#pragma unroll
+  for (int k = 0; k < 16; ++k) {
+    const c2<T> w = mk<T>(wr[k], INV ? ws[k] : -ws[k]);
+    const c2<T> t = (k == 0) ? o[k] : (k == 8 ? rot90<T, INV>(o[k]) : cmul<T>(o[k], w));
+    a[k] = cadd<T>(e[k], t);
+    a[k + 16] = csub<T>(e[k], t);
+  }
+}
+
 template <int R, typename T, bool INV> __device__ __forceinline__ void dft(c2<T>* a) {
   if constexpr (R == 2) dft2<T, INV>(a);
   else if constexpr (R == 4) dft4<T, INV>(a);
   else if constexpr (R == 8) dft8<T, INV>(a);
   else if constexpr (R == 16) dft16<T, INV>(a);
-  else static_assert(R == 2 || R == 4 || R == 8 || R == 16, "unsupported radix");
+  else if constexpr (R == 32) dft32<T, INV>(a);
+  else static_assert(R == 2 || R == 4 || R == 8 || R == 16 || R == 32, "unsupported radix");
 }
 
 // ------------------------------------------------------------ tile layout
@@ -360,6 +391,47 @@ __device__ __forceinline__ void sp_write(c2<T>* buf, c2<T> (&v)[SpGeom<L, R, LIN
   sp_emit<T, L, R, NS, LINES, NT>(v, [=](int m, int line, c2<T> x) { buf[sw<T, LINES>(m, line)] = x; }, tid);
 }
 
+// Two-pass form of fft_mul_ifft for a plan L = R1 x R2: the forward pass 2
+// (radix R2 after R1, twiddles ``twf``), ``mul``, the inverse pass 1 (radix
+// R2, no twiddles) in registers, then the inverse pass 2 (radix R1 after R2,
+// twiddles ``twi``).  Shared memory sees one store and one load of the tile
+// per direction.  ``twf`` and ``twi`` are pass-table blocks: W^{r k} at
+// (r - 1) NS + k.
+template <typename T, int L, int R1, int R2, int LINES, int NT, class Src, class Mul, class Dst>
+__device__ __forceinline__ void fft_mul_ifft_2p(c2<T>* buf, const c2<T>* twf, const c2<T>* twi, int tid, Src src,
+                                                Mul mul, Dst dst) {
+  static_assert(R1 * R2 == L, "plan");
+  auto smem = [=](int m, int line) { return buf[sw<T, LINES>(m, line)]; };
+  c2<T> a[SpGeom<L, R1, LINES, NT>::PER][R1];
+  c2<T> b[SpGeom<L, R2, LINES, NT>::PER][R2];
+  sp_read<T, L, R1, 1, LINES, NT, false, L, true>(a, src, twf, tid);
+  sp_write<T, L, R1, 1, LINES, NT>(buf, a, tid);
+  __syncthreads();
+  sp_read<T, L, R2, R1, LINES, NT, false, L, true>(b, smem, twf, tid);
+  sp_apply<T, L, R2, R1, LINES, NT>(b, mul, tid);
+#pragma unroll
+  for (int i = 0; i < SpGeom<L, R2, LINES, NT>::PER; ++i) {
+    if (SpGeom<L, R2, LINES, NT>::TOT % NT == 0 || tid + i * NT < SpGeom<L, R2, LINES, NT>::TOT)
+      dft<R2, T, true>(b[i]);
+  }
+  __syncthreads();
+  sp_write<T, L, R2, 1, LINES, NT>(buf, b, tid);
+  __syncthreads();
+  sp_read<T, L, R1, R2, LINES, NT, true, L, true>(a, smem, twi, tid);
+  sp_emit<T, L, R1, R2, LINES, NT>(a, dst, tid);
+}
+
+// Column table: the two-pass plan 512 = 16 x 32 of the column pass.  Block
+// (R 32, NS 16) of the forward pass 2 at entry 0, block (R 16, NS 32) of the
+// inverse pass 2 after it; lengths without a two-pass column plan have none.
+__host__ __device__ constexpr bool col2_plan(int L) { return L == 512; }
+__host__ __device__ constexpr int col2_r1(int) { return 16; }
+__host__ __device__ constexpr int col2_r2(int) { return 32; }
+__host__ __device__ constexpr int ctw_inv_offset(int L) { return col2_plan(L) ? (col2_r2(L) - 1) * col2_r1(L) : 0; }
+__host__ __device__ constexpr int ctw_size(int L) {
+  return col2_plan(L) ? ctw_inv_offset(L) + (col2_r1(L) - 1) * col2_r2(L) : 0;
+}
+
 // src -> FFT -> mul -> IFFT -> dst for the LINES lines of one tile, with the
 // forward plan's last pass and the inverse plan's first pass fused in
 // registers.  The inverse runs the forward radices in reverse order, so both
@@ -383,24 +455,7 @@ __device__ __forceinline__ void fft_mul_ifft(c2<T>* buf, const c2<T>* tw, int ti
   static_assert(OF2 >= 0 && OI2 >= 0 && (R3 == 1 || (OF3 >= 0 && OI3 >= 0)), "pass table block missing");
   static_assert(L == 32 || L == 64 || L == 128 || L == 256 || L == 512 || L == 1024, "unsupported length");
   if constexpr (R3 == 1) {
-    static_assert(R1 * R2 == L, "plan");
-    c2<T> a[SpGeom<L, R1, LINES, NT>::PER][R1];
-    c2<T> b[SpGeom<L, R2, LINES, NT>::PER][R2];
-    sp_read<T, L, R1, 1, LINES, NT, false, L, true>(a, src, tw, tid);
-    sp_write<T, L, R1, 1, LINES, NT>(buf, a, tid);
-    __syncthreads();
-    sp_read<T, L, R2, R1, LINES, NT, false, L, true>(b, smem, tw + OF2, tid);
-    sp_apply<T, L, R2, R1, LINES, NT>(b, mul, tid);
-#pragma unroll
-    for (int i = 0; i < SpGeom<L, R2, LINES, NT>::PER; ++i) {
-      if (SpGeom<L, R2, LINES, NT>::TOT % NT == 0 || tid + i * NT < SpGeom<L, R2, LINES, NT>::TOT)
-        dft<R2, T, true>(b[i]);
-    }
-    __syncthreads();
-    sp_write<T, L, R2, 1, LINES, NT>(buf, b, tid);
-    __syncthreads();
-    sp_read<T, L, R1, R2, LINES, NT, true, L, true>(a, smem, tw + OI2, tid);
-    sp_emit<T, L, R1, R2, LINES, NT>(a, dst, tid);
+    fft_mul_ifft_2p<T, L, R1, R2, LINES, NT>(buf, tw + OF2, tw + OI2, tid, src, mul, dst);
   } else {
     static_assert(R1 * R2 * R3 == L, "plan");
     c2<T> a[SpGeom<L, R1, LINES, NT>::PER][R1];

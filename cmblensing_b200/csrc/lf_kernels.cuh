@@ -39,6 +39,7 @@ struct StageArgs {
   void* gx;  // column pass output
   const void* twN;  // N complex T, exp(-2 pi i k / N)
   const void* twP;  // pass table of length N (ptw_size(N) complex T): column pass, paired row pass
+  const void* twC;  // column table of the two-pass column plan (ctw_size(N) complex T; N = 512)
   double kbase;     // 2 pi / (N d)
   double t_cur;     // time of the rate evaluated in this stage
   double t_next;    // time of the next stage input
@@ -114,24 +115,30 @@ __device__ __forceinline__ void load_twiddles(c2<T>* tw, const void* g, int tid)
   for (int i = tid; i < N; i += NT) tw[i] = src[i];
 }
 
-// shared-memory entries reserved for the column pass's pass table (rounded
-// up to an even count so that the tile after it stays 16-byte aligned)
-__host__ __device__ constexpr int col_tw_entries(int n) { return (ptw_size(n) + 1) & ~1; }
+// shared-memory entries reserved for the column pass's twiddle table (rounded
+// up to an even count so that the tile after it stays 16-byte aligned); TWO:
+// the column table of the two-pass plan
+__host__ __device__ constexpr int col_tw_entries(int n, bool two = false) {
+  return ((two ? ctw_size(n) : ptw_size(n)) + 1) & ~1;
+}
 
 // ======================================================== column pass
 // Gx = IFFT_col( (i KX / N^2) * FFT_col(S) ) on tiles of LINES columns.
-// grid: x = column tile (N/2/LINES), y = plane.
-template <typename T, int N, int LINES, int NT, int MINB = 1>
+// grid: x = column tile (N/2/LINES), y = plane.  TWO: the plan N = 16 x 32
+// (one shared-memory round trip per direction) instead of 8 x 8 x 8.
+template <typename T, int N, int LINES, int NT, int MINB = 1, bool TWO = false>
 __global__ void __launch_bounds__(NT, MINB) k_col(StageArgs a) {
   constexpr int H = N / 2;
+  static_assert(!TWO || col2_plan(N), "no two-pass column plan for this length");
   extern __shared__ __align__(16) unsigned char smem_raw[];
-  c2<T>* tw = reinterpret_cast<c2<T>*>(smem_raw);  // pass table
-  c2<T>* buf = tw + col_tw_entries(N);
+  c2<T>* tw = reinterpret_cast<c2<T>*>(smem_raw);  // pass table or column table
+  c2<T>* buf = tw + col_tw_entries(N, TWO);
   const int tid = threadIdx.x;
   const int c0 = blockIdx.x * LINES;
   const long plane = blockIdx.y;
   static_assert(H % LINES == 0, "column tiles must cover the packed spectrum");
-  load_twiddles<T, ptw_size(N), NT>(tw, a.twP, tid);
+  if constexpr (TWO) load_twiddles<T, ctw_size(N), NT>(tw, a.twC, tid);
+  else load_twiddles<T, ptw_size(N), NT>(tw, a.twP, tid);
   const c2<T>* in = reinterpret_cast<const c2<T>*>(a.s) + plane * (long)N * H + c0;
   c2<T>* out = reinterpret_cast<c2<T>*>(a.gx) + plane * (long)N * H + c0;
   // i KX / N^2 between the transforms; zero on KX's Nyquist row of the packed
@@ -145,7 +152,10 @@ __global__ void __launch_bounds__(NT, MINB) k_col(StageArgs a) {
   // rows of LINES consecutive columns: each warp's accesses cover whole 128-byte lines
   auto src = [=](int m, int line) { return in[m * H + line]; };
   auto dst = [=](int m, int line, c2<T> x) { out[m * H + line] = x; };
-  fft_mul_ifft<T, N, LINES, NT>(buf, tw, tid, src, kx_mul, dst);
+  if constexpr (TWO)
+    fft_mul_ifft_2p<T, N, col2_r1(N), col2_r2(N), LINES, NT>(buf, tw, tw + ctw_inv_offset(N), tid, src, kx_mul, dst);
+  else
+    fft_mul_ifft<T, N, LINES, NT>(buf, tw, tid, src, kx_mul, dst);
 }
 
 // ========================================================= row pass
