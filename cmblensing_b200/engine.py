@@ -221,6 +221,19 @@ class Plan:
         return ms.value, n.value
 
 
+def chunk_schedule(batch, chunks=16, chunk_sizes=None):
+    """Chunk sizes of a HostPipeline call: ``chunk_sizes`` as given (positive, summing to ``batch``), else
+    ``chunks`` near-equal chunks (the last may be shorter)."""
+    if chunk_sizes is None:
+        k = max(1, min(int(chunks), batch))
+        step = max(1, -(-batch // k))
+        chunk_sizes = [min(step, batch - lo) for lo in range(0, batch, step)]
+    chunk_sizes = [int(c) for c in chunk_sizes]
+    if any(c <= 0 for c in chunk_sizes) or sum(chunk_sizes) != batch:
+        raise ValueError(f"chunk sizes {chunk_sizes} must be positive and sum to the batch {batch}")
+    return chunk_sizes
+
+
 class HostPipeline:
     """The reference-facing call with host buffers, for a fixed batch, pipelined.
 
@@ -246,13 +259,16 @@ class HostPipeline:
     """
 
     def __init__(self, plan, batch, io_dtype=torch.float64, chunks=16, compute_streams=2, slots=4,
-                 use_graphs=True):
+                 use_graphs=True, chunk_sizes=None):
         self.plan = plan
         N, C = plan.nside, plan.ncomp
         dev = plan.device
         self.batch = batch
-        self.chunks = max(1, min(int(chunks), batch))
-        self.cb = -(-batch // self.chunks)  # maps per chunk (last may be shorter)
+        chunk_sizes = chunk_schedule(batch, chunks, chunk_sizes)
+        self.sizes = chunk_sizes
+        self.offsets = [sum(chunk_sizes[:i]) for i in range(len(chunk_sizes))]
+        self.chunks = len(chunk_sizes)
+        self.cb = max(chunk_sizes, default=1)  # device buffers hold the largest chunk
         cb = self.cb
         self.io_dtype = io_dtype
         self.nslots = max(2, int(slots))
@@ -264,7 +280,7 @@ class HostPipeline:
         self.ws = [torch.empty(16, dtype=torch.uint8, device=dev) for _ in range(ns)]  # sized for n at first call
         self.phi_ws = [torch.empty(max(plan.phi_workspace_bytes(cb), 16), dtype=torch.uint8, device=dev)
                        for _ in range(ns)]
-        self.min_det = torch.empty(max(self.chunks * cb, 1), dtype=torch.int32, device=dev)
+        self.min_det = torch.empty(max(batch, 1), dtype=torch.int32, device=dev)
         self.s_in = torch.cuda.Stream(dev)
         self.s_cmp = [torch.cuda.Stream(dev) for _ in range(max(1, int(compute_streams)))]
         self.s_out = torch.cuda.Stream(dev)
@@ -315,10 +331,8 @@ class HostPipeline:
         ev_out = [torch.cuda.Event() for _ in range(self.chunks)]
         ns = self.nslots
         for i in range(self.chunks):
-            lo, hi = i * self.cb, min((i + 1) * self.cb, self.batch)
-            m = hi - lo
-            if m <= 0:
-                break
+            lo, m = self.offsets[i], self.sizes[i]
+            hi = lo + m
             slot = i % ns
             with torch.cuda.stream(self.s_in):
                 if i >= ns:

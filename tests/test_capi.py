@@ -73,3 +73,16 @@ def test_encoded_order_is_monotone():
         bits = struct.unpack("<i", struct.pack("<f", v))[0]
         enc.append(bits if bits >= 0 else bits ^ 0x7FFFFFFF)
     assert enc == sorted(enc)
+
+
+def test_host_pipeline_chunk_schedule():
+    """Chunk sizes of the pipelined host-buffer call: near-equal by default, validated when given."""
+    from cmblensing_b200.engine import chunk_schedule
+    assert chunk_schedule(64, 16) == [4] * 16
+    assert chunk_schedule(5, 2) == [3, 2]
+    assert chunk_schedule(3, 16) == [1, 1, 1]
+    assert chunk_schedule(0, 16) == []
+    assert chunk_schedule(8, 4, [1, 2, 4, 1]) == [1, 2, 4, 1]
+    for bad in ([1, 2, 4], [0, 4, 4], [9, -1]):
+        with pytest.raises(ValueError):
+            chunk_schedule(8, 4, bad)

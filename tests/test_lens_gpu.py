@@ -318,19 +318,20 @@ def test_reference_shaped_api(torch_cuda):
     assert rel_l2(out.polar_matrix_2, ref[1]) < TOL32
 
 
-@pytest.mark.parametrize("B,chunks", [(5, 2), (8, 4)])
-def test_host_pipeline_matches_device_call(torch_cuda, B, chunks):
+@pytest.mark.parametrize("B,chunks,sizes", [(5, 2, None), (8, 4, None), (8, 4, [1, 2, 4, 1])])
+def test_host_pipeline_matches_device_call(torch_cuda, B, chunks, sizes):
     """The pipelined host-buffer path (three streams, double-buffered chunks) equals the device call per map."""
     import torch
     from cmblensing_b200 import engine
     f, phis = _inputs(128, 3.0, 2, B=B)
     pw = R.pix_width_of(3.0)
     plan = engine.get_plan(128, 2, pw)
-    pipe = engine.HostPipeline(plan, B, chunks=chunks)
+    pipe = engine.HostPipeline(plan, B, chunks=chunks, chunk_sizes=sizes)
     fh = torch.from_numpy(f).pin_memory()
     ph = torch.from_numpy(phis).pin_memory()
     oh = torch.empty_like(fh).pin_memory()
-    for _ in range(2):  # second call reuses every slot
+    for _ in range(3):  # eager, graph capture, graph replay; every slot reused
+        oh.zero_()
         pipe(fh, ph, oh, n=7)
         torch.cuda.synchronize()
     ref = plan.lense_flow(torch.as_tensor(f, device="cuda"), plan.phi_planes(torch.as_tensor(phis, device="cuda")),
