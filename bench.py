@@ -18,6 +18,8 @@ than the 126 MB L2, so no flush is needed between steps.
              average event-timed duration inside the timed region.
 Multi-GPU: every rank lenses its own batch (no collective; weak scaling).
 ``--impl reference`` times the float64 CPU oracle on the host cores instead.
+``--adjoint`` measures the adjoint lens (the transpose, run by every Wiener
+filter iteration and gradient) on the same workload instead of the forward.
 """
 import argparse
 import json
@@ -32,6 +34,7 @@ ROOT = os.path.dirname(os.path.abspath(__file__))
 sys.path.insert(0, ROOT)
 
 METRIC = "LenseFlow 512x512 QU maps/s (FP32, nsteps=7, incl. phi precompute)"
+METRIC_ADJ = "LenseFlow 512x512 QU adjoint maps/s (FP32, nsteps=7, incl. phi precompute)"
 UNIT = "maps/s"
 
 
@@ -51,13 +54,19 @@ def parse():
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--serving-seconds", type=float, default=1.5)
     ap.add_argument("--serving-rate", type=float, default=200.0)
+    ap.add_argument("--adjoint", action="store_true", help="time the adjoint lens instead of the forward lens")
     return ap.parse_args()
 
 
+def metric_name(a):
+    return METRIC_ADJ if a.adjoint else METRIC
+
+
 def workload_config(a):
-    return {"workload": f"lenseflow_fwd_qu{a.nside}_b{a.batch}_n{a.nsteps}" if a.ncomp == 2 else
-            f"lenseflow_fwd_c{a.ncomp}_{a.nside}_b{a.batch}_n{a.nsteps}",
-            "nside": a.nside, "ncomp": a.ncomp, "batch_per_gpu": a.batch, "rk4_steps": a.nsteps,
+    kind = "adj" if a.adjoint else "fwd"
+    return {"workload": f"lenseflow_{kind}_qu{a.nside}_b{a.batch}_n{a.nsteps}" if a.ncomp == 2 else
+            f"lenseflow_{kind}_c{a.ncomp}_{a.nside}_b{a.batch}_n{a.nsteps}",
+            "adjoint": bool(a.adjoint), "nside": a.nside, "ncomp": a.ncomp, "batch_per_gpu": a.batch, "rk4_steps": a.nsteps,
             "theta_pix_arcmin": a.theta,
             "phi_spectrum": "1/[l^2 (l+1)^2 (1+(l/60)^2)], 2.5' rms deflection (well-posed reading)",
             "fields": "QU from E ~ l^-2 exp(-(l/2000)^2), 5 uK rms, B=0" if a.ncomp == 2 else "T",
@@ -72,13 +81,13 @@ def _cpu_lens_one(args):
     sys.path.insert(0, ROOT)
     from oracle import lenseflow_ref as R
     from cmblensing_b200.simulate import lens_batch
-    N, theta, C, n, seed = args
+    N, theta, C, n, seed, adjoint = args
     f, phis = lens_batch(N, theta, 1, C, seed0=seed)
     pw = R.pix_width_of(theta)
     d = R.phi_derivatives(phis[0], pw)
     t0 = time.perf_counter()
     for c in range(C):
-        R.primal_lense_flow(f[0, c], phis[0], pw, n, 1, False, d)
+        R.primal_lense_flow(f[0, c], phis[0], pw, n, 1, adjoint, d)
     return time.perf_counter() - t0
 
 
@@ -96,7 +105,7 @@ class CpuPool:
         The time is the slowest worker's lens time: input generation, done in
         the workers before their clocks start, is excluded.
         """
-        jobs = [(a.nside, a.theta, a.ncomp, a.nsteps, seed + i) for i in range(nmaps)]
+        jobs = [(a.nside, a.theta, a.ncomp, a.nsteps, seed + i, bool(a.adjoint)) for i in range(nmaps)]
         per = self.pool.map(_cpu_lens_one, jobs, chunksize=1)
         waves = math.ceil(nmaps / self.cores)
         return max(per) * waves, sum(per)
@@ -138,7 +147,7 @@ def run_reference(a):
     value = nmaps * a.steps / total
     sample = (f"{nmaps} maps per step ({a.nside}^2, C={a.ncomp}, n={a.nsteps}, float64 numpy oracle, "
               f"one map per process), {pool.cores} processes on {cpu_describe()}")
-    line = {"impl": "reference", "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": a.gpus,
+    line = {"impl": "reference", "metric": metric_name(a), "value": value, "unit": UNIT, "n_gpus": a.gpus,
             "steps": a.steps, "warmup": a.warmup, "ms_per_step": 1000 * total / a.steps, "higher_is_better": True,
             "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
             "config": workload_config(a),
@@ -214,28 +223,34 @@ def aggregate_value(world, batch_per_rank, steps, ms):
 
 
 # ----------------------------------------------------------- algorithmic bytes
-def row_bytes_per_lens(C, n, P, in_bytes=4, out_bytes=4, p_planes=2):
-    """Bytes the row kernels of one forward lens must move per map (float32 state).
+def row_bytes_per_lens(C, n, P, in_bytes=4, out_bytes=4, p_planes=2, adjoint=False):
+    """Bytes the row kernels of one lens must move per map (float32 state).
 
-    init: read f, write y0 and S.  Stage 1: read Gx, S, y0, the phi planes;
-    write acc, S.  Stages 2-3: also read acc.  Stage 4: read Gx, S, y0, acc,
-    phi planes; write y0 and S (the last stage writes the output instead and
-    no S).  ``p_planes`` = 2 when p is read at the stage time, 5 when it is
-    formed from the derivative planes.
+    Forward -- init: read f, write y0 and S.  Stage 1: read Gx, S, y0, the phi
+    planes; write acc, S.  Stages 2-3: also read acc.  Stage 4: read Gx, S,
+    y0, acc, phi planes; write y0 and S (the last stage writes the output
+    instead and no S).  Adjoint -- the same with V read in place of S, and
+    both U and V written (init: read f, the p planes; write y0, U, V).
+    ``p_planes`` = 2 when p is read at the stage time, 5 when it is formed
+    from the derivative planes.
     """
     ph = 4 * p_planes
-    init = (in_bytes + 8) * C
-    s1 = 20 * C + ph
-    s23 = 24 * C + ph
-    s4 = 24 * C + ph
-    last_adj = -8 * C + out_bytes * C  # last stage: no y0/S writes, one output write
+    w = 8 if adjoint else 4  # next-stage spectra written per component
+    init = (in_bytes + 4 + w) * C + (ph if adjoint else 0)
+    s1 = 16 * C + w * C + ph
+    s23 = 20 * C + w * C + ph
+    s4 = 20 * C + w * C + ph
+    last_adj = -(4 + w) * C + out_bytes * C  # last stage: no y0/spectra writes, one output write
     total = init + n * (s1 + 2 * s23 + s4) + last_adj
     return total * P
 
 
-def row_kernel_name(N, C):
-    """The stage row-pass kernel the engine launches for a forward lens of this shape."""
+def row_kernel_name(N, C, adjoint=False):
+    """The stage row-pass kernel the engine launches for a lens of this shape."""
     if N == 512 and C == 2:
+        if adjoint:
+            return ("k_row_pair_adj (adjoint RK4 row pass, both rates from one full-length complex transform, "
+                    "update in registers)")
         return "k_row_pair (RK4 row pass, two components in full-length complex transforms, update in registers)"
     return "k_row (RK4 row pass + fused epilogue)"
 
@@ -243,6 +258,23 @@ def row_kernel_name(N, C):
 def col_bytes_per_lens(C, n, P):
     """Column kernels: read and write one row-spectral array (N x N/2 complex64 = 4P bytes) per plane."""
     return 4 * n * 8 * C * P
+
+
+# DRAM bytes (dram__bytes_read.sum + dram__bytes_write.sum) per map of one RK4
+# stage-1 launch of the dominant row kernel (the 13th launch of the kernel in
+# a 16-map step: RK4 step 4, stage 1), from one ncu capture each; the capture's
+# traffic scales with the maps of the launch.  The algorithmic bytes of that
+# launch are stage1_bytes_per_map(C) N^2; the reads equal them, the writes
+# fall short by what is still in L2 when the launch ends.
+NCU_STAGE1_TRAFFIC_PER_MAP = {
+    ("k_row_pair", 512, 2): (134.28e6 + 30.16e6) / 16,
+    ("k_row_pair_adj", 512, 2): (134.27e6 + 53.81e6) / 16,
+}
+
+
+def stage1_bytes_per_map(C, adjoint=False):
+    """Algorithmic bytes per N^2 of one stage-1 row launch (see row_bytes_per_lens)."""
+    return (24 if adjoint else 20) * C + 8
 
 
 def p_plane_bytes_per_lens(n, P):
@@ -402,12 +434,12 @@ def main():
     phi_dev = torch.as_tensor(phi_host, device=dev)
     out_dev = torch.empty_like(f_dev)
     planes = torch.empty((B, 5, N, N), dtype=torch.float32, device=dev)
-    ws = torch.empty(plan.workspace_bytes(B, False, n), dtype=torch.uint8, device=dev)
+    ws = torch.empty(plan.workspace_bytes(B, a.adjoint, n), dtype=torch.uint8, device=dev)
     phi_ws = torch.empty(plan.phi_workspace_bytes(B), dtype=torch.uint8, device=dev)
 
     def step():
         plan.phi_planes(phi_dev, check_det=False, out=planes, workspace=phi_ws)
-        plan.lense_flow(f_dev, planes, n=n, out=out_dev, workspace=ws)
+        plan.lense_flow(f_dev, planes, n=n, adjoint=a.adjoint, out=out_dev, workspace=ws)
 
     # the magnification check once, outside the timed region
     plan.phi_planes(phi_dev[:uniq], check_det=True)
@@ -451,25 +483,32 @@ def main():
     hbm_peak = float(peaks.get("hbm_gbs", 6650.0))
     peak_src = "measured" if "hbm_gbs" in peaks else "fallback"
 
-    row_b = row_bytes_per_lens(C, n, P, 4, 4) * B / max(4 * n + 1, 1)  # per launch, all maps
+    row_b = row_bytes_per_lens(C, n, P, 4, 4, adjoint=a.adjoint) * B / max(4 * n + 1, 1)  # per launch, all maps
     col_b = col_bytes_per_lens(C, n, P) * B / max(4 * n, 1)
     kinds = {"row": (row_ms, row_n, row_b), "col": (col_ms, col_n, col_b)}
     dom = max(kinds, key=lambda k: kinds[k][0])
     k_ms, k_n, k_b = kinds[dom]
     avg_s = (k_ms / max(k_n, 1)) / 1000.0
     achieved = k_b / avg_s / 1e9 if avg_s > 0 else 0.0
+    kname = row_kernel_name(N, C, a.adjoint) if dom == "row" else "k_col (column FFT pass)"
+    t_map = NCU_STAGE1_TRAFFIC_PER_MAP.get((kname.split()[0], N, C)) if dom == "row" else None
+    traffic = t_map * B if t_map is not None else None
     step_gbs = survey_bytes_per_map(C, n, P) * (value / world) / 1e9
     # the bytes this engine's path moves per map: row + column passes, phi
     # precompute and the stage-time p planes
-    path_b = row_bytes_per_lens(C, n, P) + col_bytes_per_lens(C, n, P) + 140 * P + p_plane_bytes_per_lens(n, P)
+    path_b = (row_bytes_per_lens(C, n, P, adjoint=a.adjoint) + col_bytes_per_lens(C, n, P) + 140 * P
+              + p_plane_bytes_per_lens(n, P))
     path_gbs = path_b * (value / world) / 1e9
 
-    result = {"metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": a.steps,
+    result = {"metric": metric_name(a), "value": value, "unit": UNIT, "n_gpus": world, "steps": a.steps,
               "warmup": a.warmup, "ms_per_step": ms / a.steps, "higher_is_better": True, "scaling": "weak",
               "vs_baseline": None, "dtype": "f32", "data": "synthetic", "config": workload_config(a),
-              "roofline": {"bound": "hbm", "kernel": row_kernel_name(N, C) if dom == "row"
-                           else "k_col (column FFT pass)", "achieved": achieved, "peak": hbm_peak,
-                           "unit": "GB/s", "frac": achieved / hbm_peak, "traffic": None,
+              "roofline": {"bound": "hbm", "kernel": kname, "achieved": achieved, "peak": hbm_peak,
+                           "unit": "GB/s", "frac": achieved / hbm_peak, "traffic": traffic,
+                           "traffic_launch": "RK4 stage 1 (ncu, 16-map capture scaled to the batch)"
+                           if traffic is not None else None,
+                           "traffic_launch_algorithmic_bytes": stage1_bytes_per_map(C, a.adjoint) * P * B
+                           if traffic is not None else None,
                            "peak_source": peak_src,
                            "bytes_per_launch": k_b, "avg_launch_ms": avg_s * 1000.0,
                            "step_model_gbs": step_gbs, "step_model_frac": step_gbs / hbm_peak,
@@ -487,14 +526,14 @@ def main():
         ph = torch.from_numpy(phi_host).pin_memory()
         oh = torch.empty_like(fh).pin_memory()
         for _ in range(max(a.warmup, 1)):
-            pipe(fh, ph, oh, n=n)
+            pipe(fh, ph, oh, n=n, adjoint=a.adjoint)
         torch.cuda.synchronize()
         barrier()
         e0 = torch.cuda.Event(enable_timing=True)
         e1 = torch.cuda.Event(enable_timing=True)
         e0.record()
         for _ in range(a.steps):
-            pipe(fh, ph, oh, n=n)
+            pipe(fh, ph, oh, n=n, adjoint=a.adjoint)
         e1.record()
         barrier()
         ems = max_over_ranks(e0.elapsed_time(e1), dist, dev)
@@ -506,7 +545,7 @@ def main():
         result["e2e"]["rel_l2_vs_device_leg"] = diff
 
     # ---------------------------------------------------- FP64 comparator
-    if not a.no_fp64 and rank == 0:
+    if not a.no_fp64 and not a.adjoint and rank == 0:  # the float64 restatement is forward-only
         sys.path.insert(0, os.path.join(ROOT, "baseline"))
         from fp64_torch import lense_flow_fp64
         nb = 4

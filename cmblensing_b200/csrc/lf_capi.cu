@@ -159,6 +159,7 @@ cudaError_t launch_col(int planes, cudaStream_t st, const StageArgs& a) {
   constexpr int LINES = Geo<T>::LINES;
   const dim3 grid(N / 2 / LINES, planes);
   if constexpr (std::is_same<T, float>::value && col2_plan(N)) {
+    // 16-line tiles (128-byte row segments), 256 threads (one radix-32 butterfly each), 2 blocks per SM
     constexpr int NT2 = 256;
     const size_t smem = sizeof(c2<T>) * (col_tw_entries(N, true) + LINES * N);
     return launch_k<k_col<T, N, LINES, NT2, 2, true>>(LF_KIND_COL, grid, NT2, smem, st, a);
