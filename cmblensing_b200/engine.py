@@ -251,11 +251,19 @@ class HostPipeline:
     first runs eagerly, which also sets the kernels' shared-memory limits) and
     replayed from then on; the capture synchronises the device once.  For 64
     512^2 QU maps with float64 host I/O: 4,528 maps/s on one stream, 5,600
-    with two compute streams, 6,411 with graphs (same outputs bit for bit).
-    The magnification minima are read back once per call, after the last
-    chunk; a call whose phi is singular raises SingularMagnificationError (its
-    outputs are then meaningless).  Device buffers are allocated once (the
-    lens workspace at the first call, when n is known).
+    with two compute streams, 6,411 with graphs, 7,240 with consecutive calls
+    queued (``wait=False``) so that each call's fill and drain overlap its
+    neighbours (same outputs bit for bit).
+    The magnification minima are read back after the last chunk; a call
+    whose phi is singular raises SingularMagnificationError (its outputs are
+    then meaningless).  ``wait=False`` returns once the call is queued: the
+    next call's first copies then overlap this call's last chunks (each
+    slot's reuse waits for the events of its previous use), and ``wait()``
+    joins the pipeline into the current stream, reads the pending minima and
+    raises for a singular phi.  The minima of the two most recent calls are
+    kept in a ring, so a third call first waits for the oldest.  Device
+    buffers are allocated once (the lens workspace at the first call, when n
+    is known).
     """
 
     def __init__(self, plan, batch, io_dtype=torch.float64, chunks=16, compute_streams=2, slots=4,
@@ -280,7 +288,13 @@ class HostPipeline:
         self.ws = [torch.empty(16, dtype=torch.uint8, device=dev) for _ in range(ns)]  # sized for n at first call
         self.phi_ws = [torch.empty(max(plan.phi_workspace_bytes(cb), 16), dtype=torch.uint8, device=dev)
                        for _ in range(ns)]
-        self.min_det = torch.empty(max(batch, 1), dtype=torch.int32, device=dev)
+        # magnification minima of the two most recent calls
+        self.min_det = [torch.empty(max(batch, 1), dtype=torch.int32, device=dev) for _ in range(2)]
+        self._ring = 0
+        self._pending = {}  # ring index -> events that end the call's compute
+        # per slot: the last compute that read its inputs, the last copy-out of its output
+        self._slot_in_free = [None] * ns
+        self._slot_out_free = [None] * ns
         self.s_in = torch.cuda.Stream(dev)
         self.s_cmp = [torch.cuda.Stream(dev) for _ in range(max(1, int(compute_streams)))]
         self.s_out = torch.cuda.Stream(dev)
@@ -289,10 +303,10 @@ class HostPipeline:
         self.graphs = {}
         self._warm = set()
 
-    def _compute(self, slot, lo, m, n, direction, adjoint, check_det):
+    def _compute(self, slot, lo, m, n, direction, adjoint, check_det, ring):
         plan, lib = self.plan, self.plan._lib
         st = _stream_ptr(plan.device)
-        md = _ptr(self.min_det[lo:]) if check_det else None
+        md = _ptr(self.min_det[ring][lo:]) if check_det else None
         nat.check(lib.lf_phi_precompute(plan.handle, _ptr(self.d_phi[slot]), nat.LF_PHI_MAP, m,
                                         _ptr(self.planes[slot]), md, _ptr(self.phi_ws[slot]),
                                         self.phi_ws[slot].numel(), st), "lf_phi_precompute")
@@ -309,7 +323,34 @@ class HostPipeline:
         N, C = self.plan.nside, self.plan.ncomp
         return self.batch * C * N * N * torch.tensor([], dtype=self.io_dtype).element_size()
 
-    def __call__(self, f_host, phi_host, out_host, n=10, direction=FORWARD_LENSE, adjoint=False, check_det=True):
+    def _check(self, ring):
+        """Read the minima of a finished call (synchronises on its compute) and raise if singular."""
+        events = self._pending.pop(ring)
+        for ev in events:
+            ev.synchronize()
+        lib = self.plan._lib
+        vals = [lib.lf_decode_min_det(int(v)) for v in self.min_det[ring][:self.batch].cpu().tolist()]
+        self.plan.last_min_det = vals
+        if not all(v > 0.0 for v in vals):
+            raise nat.SingularMagnificationError(nat.LF_ERR_SINGULAR_MAGNIFICATION,
+                                                 f"min det(I + t grad grad phi) = {min(vals):.3g}")
+
+    def wait(self):
+        """Join the queued calls into the current stream; raise for a singular phi among them."""
+        cur = torch.cuda.current_stream(self.plan.device)
+        for st in [self.s_in, self.s_out] + self.s_cmp:
+            cur.wait_stream(st)
+        err = None
+        for ring in sorted(self._pending):
+            try:
+                self._check(ring)
+            except nat.SingularMagnificationError as e:
+                err = err or e
+        if err is not None:
+            raise err
+
+    def __call__(self, f_host, phi_host, out_host, n=10, direction=FORWARD_LENSE, adjoint=False, check_det=True,
+                 wait=True):
         plan, lib = self.plan, self.plan._lib
         need = plan.workspace_bytes(self.cb, True, n)
         for k in range(self.nslots):
@@ -319,33 +360,35 @@ class HostPipeline:
         streams = [self.s_in, self.s_out] + self.s_cmp
         for st in streams:
             st.wait_stream(cur)
+        ring = self._ring
+        self._ring = 1 - ring
+        if ring in self._pending:  # the call two back is still unread
+            self._check(ring)
         first = self.s_cmp[0]
         if check_det:
             with torch.cuda.stream(first):
-                nat.check(lib.lf_min_det_init(_ptr(self.min_det), self.min_det.numel(), _stream_ptr(plan.device)),
-                          "lf_min_det_init")
+                nat.check(lib.lf_min_det_init(_ptr(self.min_det[ring]), self.min_det[ring].numel(),
+                                              _stream_ptr(plan.device)), "lf_min_det_init")
             for st in self.s_cmp[1:]:
                 st.wait_stream(first)
-        ev_in = [torch.cuda.Event() for _ in range(self.chunks)]
-        ev_cmp = [torch.cuda.Event() for _ in range(self.chunks)]
-        ev_out = [torch.cuda.Event() for _ in range(self.chunks)]
         ns = self.nslots
         for i in range(self.chunks):
             lo, m = self.offsets[i], self.sizes[i]
             hi = lo + m
             slot = i % ns
+            ev_in, ev_cmp, ev_out = torch.cuda.Event(), torch.cuda.Event(), torch.cuda.Event()
             with torch.cuda.stream(self.s_in):
-                if i >= ns:
-                    self.s_in.wait_event(ev_cmp[i - ns])  # the slot's previous chunk has been consumed
+                if self._slot_in_free[slot] is not None:
+                    self.s_in.wait_event(self._slot_in_free[slot])  # the slot's previous chunk has been consumed
                 self.d_f[slot][:m].copy_(f_host[lo:hi], non_blocking=True)
                 self.d_phi[slot][:m].copy_(phi_host[lo:hi], non_blocking=True)
-                ev_in[i].record(self.s_in)
+                ev_in.record(self.s_in)
             sc = self.s_cmp[i % len(self.s_cmp)]
             with torch.cuda.stream(sc):
-                sc.wait_event(ev_in[i])
-                if i >= ns:
-                    sc.wait_event(ev_out[i - ns])  # the slot's previous output has been copied out
-                args = (slot, lo, m, n, direction, adjoint, check_det)
+                sc.wait_event(ev_in)
+                if self._slot_out_free[slot] is not None:
+                    sc.wait_event(self._slot_out_free[slot])  # the slot's previous output has been copied out
+                args = (slot, lo, m, n, direction, adjoint, check_det, ring)
                 key = (i,) + args[2:]
                 g = self.graphs.get(key) if self.use_graphs else None
                 if g is None and self.use_graphs and key in self._warm:
@@ -359,19 +402,22 @@ class HostPipeline:
                 else:
                     self._compute(*args)  # eager; also sets kernel attributes before any capture
                     self._warm.add(key)
-                ev_cmp[i].record(sc)
+                ev_cmp.record(sc)
+            self._slot_in_free[slot] = ev_cmp
             with torch.cuda.stream(self.s_out):
-                self.s_out.wait_event(ev_cmp[i])
+                self.s_out.wait_event(ev_cmp)
                 out_host[lo:hi].copy_(self.d_out[slot][:m], non_blocking=True)
-                ev_out[i].record(self.s_out)
-        for st in streams:
-            cur.wait_stream(st)
+                ev_out.record(self.s_out)
+            self._slot_out_free[slot] = ev_out
         if check_det:
-            vals = [lib.lf_decode_min_det(int(v)) for v in self.min_det[:self.batch].cpu().tolist()]
-            plan.last_min_det = vals
-            if not all(v > 0.0 for v in vals):
-                raise nat.SingularMagnificationError(nat.LF_ERR_SINGULAR_MAGNIFICATION,
-                                                     f"min det(I + t grad grad phi) = {min(vals):.3g}")
+            ends = []
+            for st in self.s_cmp:
+                ev = torch.cuda.Event()
+                ev.record(st)
+                ends.append(ev)
+            self._pending[ring] = ends
+        if wait:
+            self.wait()
         return out_host
 
 

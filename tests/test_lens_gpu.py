@@ -339,6 +339,31 @@ def test_host_pipeline_matches_device_call(torch_cuda, B, chunks, sizes):
     assert torch.equal(oh, ref.cpu())
 
 
+def test_host_pipeline_overlapped_calls(torch_cuda):
+    """wait=False calls queue behind each other (slot reuse ordered by events); each output equals the device
+    call, and wait() joins them."""
+    import torch
+    from cmblensing_b200 import engine
+    f, phis = _inputs(128, 3.0, 2, B=6, seed0=11)
+    pw = R.pix_width_of(3.0)
+    plan = engine.get_plan(128, 2, pw)
+    pipe = engine.HostPipeline(plan, 3, chunks=3, slots=2)
+    halves = [(torch.from_numpy(f[k * 3:(k + 1) * 3].copy()).pin_memory(),
+               torch.from_numpy(phis[k * 3:(k + 1) * 3].copy()).pin_memory()) for k in range(2)]
+    outs = [torch.empty((3, 2, 128, 128), dtype=torch.float64).pin_memory() for _ in range(2)]
+    for rep in range(4):  # eager, capture, replay; the two rings alternate
+        for o in outs:
+            o.zero_()
+        for k in range(2):
+            pipe(halves[k][0], halves[k][1], outs[k], n=7, wait=False)
+        pipe.wait()
+        torch.cuda.synchronize()
+        for k in range(2):
+            ref = plan.lense_flow(torch.as_tensor(f[k * 3:(k + 1) * 3], device="cuda"),
+                                  plan.phi_planes(torch.as_tensor(phis[k * 3:(k + 1) * 3], device="cuda")), n=7)
+            assert torch.equal(outs[k], ref.cpu()), (rep, k)
+
+
 def test_host_pipeline_reports_singular_phi(torch_cuda):
     import torch
     from cmblensing_b200 import _native as nat
@@ -351,3 +376,8 @@ def test_host_pipeline_reports_singular_phi(torch_cuda):
     with pytest.raises(nat.SingularMagnificationError):
         pipe(torch.from_numpy(f).pin_memory(), torch.from_numpy(phis).pin_memory(),
              torch.empty(f.shape, dtype=torch.float64).pin_memory(), n=7)
+    # queued without waiting, the error surfaces at wait()
+    pipe(torch.from_numpy(f).pin_memory(), torch.from_numpy(phis).pin_memory(),
+         torch.empty(f.shape, dtype=torch.float64).pin_memory(), n=7, wait=False)
+    with pytest.raises(nat.SingularMagnificationError):
+        pipe.wait()
