@@ -845,10 +845,15 @@ __global__ void __launch_bounds__(NT) k_phi_cols_fwd(double2* __restrict__ arr, 
   store_cols<double, N, LINES, NT>(a, H + 1, c0, H + 1, buf, tid);
 }
 
-// Five derivative spectra: for j in {x, y, xx, xy, yy} apply the multiplier
-// (util.py:125-130), inverse column FFT, and write the packed row spectrum
-// (columns 0 and N/2 keep only their real parts, as irfft2 does).
-// ``spec`` is the unpacked rfft2 of phi; ``packed`` is [B][5][N][N/2] complex.
+// Five derivative spectra j in {x, y, xx, xy, yy} (util.py:125-130), each
+// written as a packed row spectrum (columns 0 and N/2 keep only their real
+// parts, as irfft2 does).  KY is constant down a column, so it commutes with
+// the inverse column FFT: three inverse transforms serve all five,
+//   G0 = IFFT_col(F):           phi_y = i KY G0,  phi_yy = -KY^2 G0
+//   G1 = IFFT_col(i KX F):      phi_x = G1,       phi_xy = i KY G1
+//   G2 = IFFT_col(-KX^2 F):     phi_xx = G2
+// (the 1/N^2 of irfft2 folded into the column multiplier).  ``spec`` is the
+// unpacked rfft2 of phi; ``packed`` is [B][5][N][N/2] complex.
 template <int N, int LINES, int NT>
 __global__ void __launch_bounds__(NT) k_phi_cols_deriv(const double2* __restrict__ spec, double2* __restrict__ packed,
                                                         const double2* __restrict__ twN, double kbase) {
@@ -862,35 +867,42 @@ __global__ void __launch_bounds__(NT) k_phi_cols_deriv(const double2* __restrict
   const double2* a = spec + map * (long)N * (H + 1);
   load_twiddles<double, N, NT>(tw, twN, tid);
   const double scale = 1.0 / (double(N) * double(N));
+  // (G, output j, KY power): KY power 0 = G itself, 1 = i KY G, 2 = -KY^2 G
+  constexpr int kOut[3][2][2] = {{{1, 1}, {4, 2}}, {{0, 0}, {3, 1}}, {{2, 0}, {-1, 0}}};
 #pragma unroll 1
-  for (int j = 0; j < 5; ++j) {
+  for (int g = 0; g < 3; ++g) {
     load_cols<double, N, LINES, NT>(buf, a, H + 1, c0, H + 1, tid);
     __syncthreads();
     for (int idx = tid; idx < N * LINES; idx += NT) {
       const int m = idx / LINES, line = idx % LINES;
-      const int col = c0 + line;
       const double kx = kbase * double(m < N / 2 ? m : m - N);
-      const double ky = (col == H) ? -kbase * double(H) : kbase * double(col);
       const double2 v = buf[sw<double, LINES>(m, line)];
       double2 r;
-      if (j == 0) r = make_double2(-kx * v.y * scale, kx * v.x * scale);
-      else if (j == 1) r = make_double2(-ky * v.y * scale, ky * v.x * scale);
-      else {
-        const double f = (j == 2 ? -kx * kx : (j == 3 ? -kx * ky : -ky * ky)) * scale;
-        r = make_double2(f * v.x, f * v.y);
-      }
+      if (g == 0) r = make_double2(scale * v.x, scale * v.y);
+      else if (g == 1) r = make_double2(-kx * v.y * scale, kx * v.x * scale);
+      else r = make_double2(-kx * kx * scale * v.x, -kx * kx * scale * v.y);
       buf[sw<double, LINES>(m, line)] = r;
     }
     __syncthreads();
     fft_tiles<double, N, LINES, 1, NT, true, N>(buf, tw, tid);
-    double2* out = packed + (map * 5 + j) * (long)N * H;
-    for (int idx = tid; idx < N * LINES; idx += NT) {
-      const int m = idx / LINES, line = idx % LINES;
-      const int col = c0 + line;
-      const double2 v = buf[sw<double, LINES>(m, line)];
-      if (col == 0) reinterpret_cast<double*>(out + (long)m * H)[0] = v.x;
-      else if (col == H) reinterpret_cast<double*>(out + (long)m * H)[1] = v.x;
-      else if (col < H) out[(long)m * H + col] = v;
+    for (int o = 0; o < 2; ++o) {
+      const int j = kOut[g][o][0], pw = kOut[g][o][1];
+      if (j < 0) continue;
+      double2* out = packed + (map * 5 + j) * (long)N * H;
+      for (int idx = tid; idx < N * LINES; idx += NT) {
+        const int m = idx / LINES, line = idx % LINES;
+        const int col = c0 + line;
+        if (col > H) continue;
+        const double ky = (col == H) ? -kbase * double(H) : kbase * double(col);
+        const double2 G = buf[sw<double, LINES>(m, line)];
+        double2 v;
+        if (pw == 0) v = G;
+        else if (pw == 1) v = make_double2(-ky * G.y, ky * G.x);
+        else v = make_double2(-ky * ky * G.x, -ky * ky * G.y);
+        if (col == 0) reinterpret_cast<double*>(out + (long)m * H)[0] = v.x;
+        else if (col == H) reinterpret_cast<double*>(out + (long)m * H)[1] = v.x;
+        else out[(long)m * H + col] = v;
+      }
     }
     __syncthreads();
   }
