@@ -105,7 +105,9 @@ template <> struct Geo<float> {
   static constexpr int nt(int n) { return n <= 64 ? 128 : (n <= 256 ? 256 : (n <= 512 ? 512 : 1024)); }
   static constexpr int minb(int n) { return 65536 / (nt(n) * 64); }
   static constexpr int row_nt(int n) { return nt(n) / 2; }
-  static constexpr int row_minb(int n) { return 65536 / (row_nt(n) * 64); }
+  // three components keep more values live in the epilogue: up to 85 registers
+  // (64 spilled 100-250 bytes per thread)
+  static constexpr int row_minb(int n, int c = 1) { return 65536 / (row_nt(n) * (c >= 3 ? 80 : 64)); }
 };
 template <> struct Geo<double> {
   static constexpr int LINES = 8;
@@ -113,7 +115,7 @@ template <> struct Geo<double> {
   static constexpr int nt(int n) { return n <= 64 ? 64 : (n <= 128 ? 128 : (n <= 512 ? 256 : 512)); }
   static constexpr int minb(int) { return 1; }
   static constexpr int row_nt(int n) { return nt(n); }
-  static constexpr int row_minb(int) { return 1; }
+  static constexpr int row_minb(int, int = 1) { return 1; }
 };
 
 // Opt in to > 48 KB of dynamic shared memory once per kernel and device.
@@ -174,7 +176,7 @@ template <typename T, int N, int C, bool ADJ, bool PP>
 cudaError_t run_lens_pp(const StageArgs& base, int B, int nsteps, double t0, double t1, cudaStream_t st) {
   constexpr int RL = Geo<T>::ROW_LINES;
   constexpr int RNT = Geo<T>::row_nt(N);
-  constexpr int RMB = Geo<T>::row_minb(N);
+  constexpr int RMB = Geo<T>::row_minb(N, C);
   constexpr int H = N / 2;
   const size_t smem_row = sizeof(c2<T>) * (N + 2 * C * RL * H);
   const dim3 grow(N / RL, B);
@@ -393,7 +395,7 @@ cudaError_t run_vjp_n(const StageArgs& af0, const StageArgs& ad0, double* dacc, 
                       double t1, cudaStream_t st) {
   constexpr int RL = Geo<T>::ROW_LINES;
   constexpr int RNT = Geo<T>::row_nt(N);
-  constexpr int RMB = Geo<T>::row_minb(N);
+  constexpr int RMB = Geo<T>::row_minb(N, C);
   constexpr int H = N / 2;
   const size_t smem_row = sizeof(c2<T>) * (N + 2 * C * RL * H);
   const dim3 grow(N / RL, B);
