@@ -443,18 +443,31 @@ __global__ void __launch_bounds__(NT, MINB) k_row_pair(StageArgs a) {
   static_assert(NB * LINES == NT, "one (row, butterfly) per thread in the fused passes");
   constexpr int TILE = LINES * N;
   constexpr int RB = LINES * N;  // floats per staged row block
+  constexpr int IT = 2 * LINES * (H / 2) / NT;  // packed element pairs per thread in the load phase
+  static_assert(2 * LINES * (H / 2) % NT == 0, "whole load-phase iterations");
   extern __shared__ __align__(16) unsigned char smem_raw[];
   c2<T>* tw = reinterpret_cast<c2<T>*>(smem_raw);
   c2<T>* buf = tw + N;                                 // tile c at buf + c * TILE
   T* stg = reinterpret_cast<T*>(buf + 2 * TILE);       // y0_0, y0_1, acc_0, acc_1, p_x, p_y
-  uint64_t* mbar = reinterpret_cast<uint64_t*>(stg + 6 * RB);
+  uint64_t* mbar = reinterpret_cast<uint64_t*>(stg + 6 * RB);  // [0]: staged update operands, [1]: spectra
   const int tid = threadIdx.x;
   const int r0 = blockIdx.x * LINES;
   const long map = blockIdx.y;
   const long prow0 = (long)r0 * N;
   const bool with_acc = a.stage > 1;
+  const long half_plane = N * (long)H;
+  auto spec = [&](void* base, int c) {
+    return reinterpret_cast<c2<T>*>(base) + (map * 2 + c) * half_plane + (long)r0 * H;
+  };
   if (tid == 0) {
     mbar_init(mbar, 1);
+    mbar_init(mbar + 1, 1);
+    // the spectra first (the transforms wait for them): Gx_c and S_c rows, packed, into tile c
+    mbar_expect_tx(mbar + 1, uint32_t(4 * LINES * H * sizeof(c2<T>)));
+    for (int c = 0; c < 2; ++c) {
+      bulk_g2s(buf + c * TILE, spec(a.gx, c), LINES * H * sizeof(c2<T>), mbar + 1);
+      bulk_g2s(buf + c * TILE + LINES * H, spec(a.s, c), LINES * H * sizeof(c2<T>), mbar + 1);
+    }
     mbar_expect_tx(mbar, uint32_t((with_acc ? 6 : 4) * RB * sizeof(T)));
     const T* pp = reinterpret_cast<const T*>(a.pp) + (map * a.pp_k + a.pp_idx) * 2 * P + prow0;
     for (int c = 0; c < 2; ++c) {
@@ -469,34 +482,48 @@ __global__ void __launch_bounds__(NT, MINB) k_row_pair(StageArgs a) {
   static_assert(ptw_size(N) <= N, "pass table of the 8x8x8 plan");
   constexpr int O8 = ptw_offset(N, R, R), O64 = ptw_offset(N, R, R * R);
   const T ky_scale = T(a.kbase / double(N));
-  const long half_plane = N * (long)H;
-  auto spec = [&](void* base, int c) {
-    return reinterpret_cast<c2<T>*>(base) + (map * 2 + c) * half_plane + (long)r0 * H;
-  };
+  __syncthreads();  // barriers initialised before anyone waits on them
+  if (!mbar_wait(mbar + 1, 0, kWaitTries)) {
+    // the spectra never arrived: record it (this launch's results are then
+    // invalid), let the copies drain, and go on so that every thread meets
+    // every barrier below
+    atomicExch(&g_lf_wait_timeouts, 1);
+    mbar_wait(mbar + 1, 0, kWaitTries);
+  }
 
   // ------------------------- load: Z_c = DX_c + i DY_c with DY = i KY S / N
   // (slot 0 of a packed spectrum holds the real DC and Nyquist bins; the d_y
-  // spectrum has none: KY's DC and Nyquist terms vanish after irfft)
+  // spectrum has none: KY's DC and Nyquist terms vanish after irfft).  The
+  // packed rows sit in tile c; all of them are read before Z overwrites it.
+  c2<T> gv[IT][2], sv[IT][2];
 #pragma unroll
-  for (int idx = tid; idx < 2 * LINES * (H / 2); idx += NT) {
-    const int t = idx % (H / 2);
-    const int rest = idx / (H / 2);
+  for (int it = 0; it < IT; ++it) {
+    const int idx = tid + it * NT;
+    const int t = idx % (H / 2), rest = idx / (H / 2);
     const int row = rest % LINES, c = rest / LINES;
-    c2<T> g[2], s[2];
-    ld2<T>(spec(a.gx, c) + row * H + 2 * t, g);
-    ld2<T>(spec(a.s, c) + row * H + 2 * t, s);
+    const c2<T>* pk = buf + c * TILE;
+    ld2<T>(pk + row * H + 2 * t, gv[it]);
+    ld2<T>(pk + LINES * H + row * H + 2 * t, sv[it]);
+  }
+  __syncthreads();
+#pragma unroll
+  for (int it = 0; it < IT; ++it) {
+    const int idx = tid + it * NT;
+    const int t = idx % (H / 2), rest = idx / (H / 2);
+    const int row = rest % LINES, c = rest / LINES;
     c2<T>* z = buf + c * TILE;
 #pragma unroll
     for (int q = 0; q < 2; ++q) {
       const int k = 2 * t + q;
+      const c2<T> g = gv[it][q], sq = sv[it][q];
       if (k == 0) {
-        z[sw<T, LINES>(0, row)] = mk<T>(g[0].x, T(0));
-        z[sw<T, LINES>(H, row)] = mk<T>(g[0].y, T(0));
+        z[sw<T, LINES>(0, row)] = mk<T>(g.x, T(0));
+        z[sw<T, LINES>(H, row)] = mk<T>(g.y, T(0));
       } else {
         const T f = ky_scale * T(k);
-        const T dyx = -f * s[q].y, dyy = f * s[q].x;  // DY = i f S
-        z[sw<T, LINES>(k, row)] = mk<T>(g[q].x - dyy, g[q].y + dyx);       // DX + i DY
-        z[sw<T, LINES>(N - k, row)] = mk<T>(g[q].x + dyy, dyx - g[q].y);   // conj(DX) + i conj(DY)
+        const T dyx = -f * sq.y, dyy = f * sq.x;  // DY = i f S
+        z[sw<T, LINES>(k, row)] = mk<T>(g.x - dyy, g.y + dyx);       // DX + i DY
+        z[sw<T, LINES>(N - k, row)] = mk<T>(g.x + dyy, dyx - g.y);   // conj(DX) + i conj(DY)
       }
     }
   }
@@ -618,18 +645,31 @@ __global__ void __launch_bounds__(NT, MINB) k_row_pair_adj(StageArgs a) {
   static_assert(NB * LINES == NT, "one (row, butterfly) per thread in the fused passes");
   constexpr int TILE = LINES * N;
   constexpr int RB = LINES * N;
+  constexpr int IT = LINES * (H / 2) / NT;  // packed element pairs per thread in the load phase
+  static_assert(LINES * (H / 2) % NT == 0, "whole load-phase iterations");
   extern __shared__ __align__(16) unsigned char smem_raw[];
   c2<T>* tw = reinterpret_cast<c2<T>*>(smem_raw);
   c2<T>* buf = tw + N;                            // Z (tile 0); then w_u (tile 0), w_v (tile 1)
   T* stg = reinterpret_cast<T*>(buf + 2 * TILE);  // y0_0, y0_1, acc_0, acc_1, p_x, p_y
-  uint64_t* mbar = reinterpret_cast<uint64_t*>(stg + 6 * RB);
+  uint64_t* mbar = reinterpret_cast<uint64_t*>(stg + 6 * RB);  // [0]: staged update operands, [1]: spectra
   const int tid = threadIdx.x;
   const int r0 = blockIdx.x * LINES;
   const long map = blockIdx.y;
   const long prow0 = (long)r0 * N;
   const bool with_acc = a.stage > 1;
+  const long half_plane = N * (long)H;
+  auto spec = [&](void* base, int c) {
+    return reinterpret_cast<c2<T>*>(base) + (map * 2 + c) * half_plane + (long)r0 * H;
+  };
   if (tid == 0) {
     mbar_init(mbar, 1);
+    mbar_init(mbar + 1, 1);
+    // the spectra first: Gx_c and V_c rows, packed, into tile c
+    mbar_expect_tx(mbar + 1, uint32_t(4 * LINES * H * sizeof(c2<T>)));
+    for (int c = 0; c < 2; ++c) {
+      bulk_g2s(buf + c * TILE, spec(a.gx, c), LINES * H * sizeof(c2<T>), mbar + 1);
+      bulk_g2s(buf + c * TILE + LINES * H, spec(a.v, c), LINES * H * sizeof(c2<T>), mbar + 1);
+    }
     mbar_expect_tx(mbar, uint32_t((with_acc ? 6 : 4) * RB * sizeof(T)));
     const T* pp = reinterpret_cast<const T*>(a.pp) + (map * a.pp_k + a.pp_idx) * 2 * P + prow0;
     for (int c = 0; c < 2; ++c) {
@@ -643,30 +683,42 @@ __global__ void __launch_bounds__(NT, MINB) k_row_pair_adj(StageArgs a) {
   load_twiddles<T, ptw_size(N), NT>(tw, a.twP, tid);
   constexpr int O8 = ptw_offset(N, R, R), O64 = ptw_offset(N, R, R * R);
   const T ky_scale = T(a.kbase / double(N));
-  const long half_plane = N * (long)H;
-  auto spec = [&](void* base, int c) {
-    return reinterpret_cast<c2<T>*>(base) + (map * 2 + c) * half_plane + (long)r0 * H;
-  };
+  __syncthreads();  // barriers initialised before anyone waits on them
+  if (!mbar_wait(mbar + 1, 0, kWaitTries)) {
+    // the spectra never arrived: record it (this launch's results are then
+    // invalid), let the copies drain, and go on so that every thread meets
+    // every barrier below
+    atomicExch(&g_lf_wait_timeouts, 1);
+    mbar_wait(mbar + 1, 0, kWaitTries);
+  }
 
   // -------------------- load: Z = K_0 + i K_1, K_c = Gx_c + i KY V_c / N (Hermitian)
+  // The packed rows sit in tiles 0 and 1; all are read before Z overwrites tile 0.
+  c2<T> g0[IT][2], g1[IT][2], v0[IT][2], v1[IT][2];
 #pragma unroll
-  for (int idx = tid; idx < LINES * (H / 2); idx += NT) {
+  for (int it = 0; it < IT; ++it) {
+    const int idx = tid + it * NT;
     const int t = idx % (H / 2), row = idx / (H / 2);
-    c2<T> g0[2], g1[2], v0[2], v1[2];
-    ld2<T>(spec(a.gx, 0) + row * H + 2 * t, g0);
-    ld2<T>(spec(a.gx, 1) + row * H + 2 * t, g1);
-    ld2<T>(spec(a.v, 0) + row * H + 2 * t, v0);
-    ld2<T>(spec(a.v, 1) + row * H + 2 * t, v1);
+    ld2<T>(buf + row * H + 2 * t, g0[it]);
+    ld2<T>(buf + LINES * H + row * H + 2 * t, v0[it]);
+    ld2<T>(buf + TILE + row * H + 2 * t, g1[it]);
+    ld2<T>(buf + TILE + LINES * H + row * H + 2 * t, v1[it]);
+  }
+  __syncthreads();
+#pragma unroll
+  for (int it = 0; it < IT; ++it) {
+    const int idx = tid + it * NT;
+    const int t = idx % (H / 2), row = idx / (H / 2);
 #pragma unroll
     for (int q = 0; q < 2; ++q) {
       const int k = 2 * t + q;
       if (k == 0) {  // real DC and Nyquist bins of each rate; i KY contributes nothing there
-        buf[sw<T, LINES>(0, row)] = mk<T>(g0[0].x, g1[0].x);
-        buf[sw<T, LINES>(H, row)] = mk<T>(g0[0].y, g1[0].y);
+        buf[sw<T, LINES>(0, row)] = mk<T>(g0[it][0].x, g1[it][0].x);
+        buf[sw<T, LINES>(H, row)] = mk<T>(g0[it][0].y, g1[it][0].y);
       } else {
         const T f = ky_scale * T(k);
-        const c2<T> k0 = mk<T>(g0[q].x - f * v0[q].y, g0[q].y + f * v0[q].x);  // Gx + i f V
-        const c2<T> k1 = mk<T>(g1[q].x - f * v1[q].y, g1[q].y + f * v1[q].x);
+        const c2<T> k0 = mk<T>(g0[it][q].x - f * v0[it][q].y, g0[it][q].y + f * v0[it][q].x);  // Gx + i f V
+        const c2<T> k1 = mk<T>(g1[it][q].x - f * v1[it][q].y, g1[it][q].y + f * v1[it][q].x);
         buf[sw<T, LINES>(k, row)] = mk<T>(k0.x - k1.y, k0.y + k1.x);            // K_0 + i K_1
         buf[sw<T, LINES>(N - k, row)] = mk<T>(k0.x + k1.y, k1.x - k0.y);        // conj(K_0) + i conj(K_1)
       }
