@@ -139,6 +139,7 @@ class DeviceWienerFilter:
         self.planes = engine.cached_phi_planes(self.plan, self.phimap)
         self.fft = engine.get_plan(N, 1, self.pw, "f64", device=dev)
         self._plan64 = None
+        self._nonzero = {}  # per-mode operator -> which of its C x C blocks are not identically zero
 
     # ----------------------------------------------------------- pieces
     @staticmethod
@@ -174,12 +175,31 @@ class DeviceWienerFilter:
             out[2, 2] = rec(P[2, 2])
         return out
 
-    @staticmethod
-    def _apply(W, X):
-        """Per-mode matrix times vector: W (C,C,N,H) shared or (B,C,C,N,H) per problem; X (B,C,N,H)."""
-        if W.dim() == 4:
-            return torch.einsum("ijnh,bjnh->binh", W, X)
-        return torch.einsum("bijnh,bjnh->binh", W, X)
+    def _apply(self, W, X):
+        """Per-mode matrix times vector: W (C,C,N,H) shared or (B,C,C,N,H) per problem; X (B,C,N,H).
+
+        Written as C x C elementwise products (memory-bound, one pass each)
+        rather than an einsum, and skipping the blocks of W that are zero
+        everywhere (an EB-diagonal operator has no off-diagonal blocks); which
+        blocks those are is found once per operator."""
+        Wb = W if W.dim() == 5 else W.unsqueeze(0)
+        C = Wb.shape[1]
+        key = (W.data_ptr(), tuple(W.shape))
+        nz = self._nonzero.get(key)
+        if nz is None:
+            nz = [[bool(torch.any(Wb[:, i, j] != 0)) for j in range(C)] for i in range(C)]
+            self._nonzero[key] = nz
+        out = torch.empty(X.shape, dtype=torch.result_type(Wb, X), device=X.device)
+        for i in range(C):
+            terms = [j for j in range(C) if nz[i][j]]
+            if not terms:
+                out[:, i] = 0
+                continue
+            acc = Wb[:, i, terms[0]] * X[:, terms[0]]
+            for j in terms[1:]:
+                acc = acc + Wb[:, i, j] * X[:, j]
+            out[:, i] = acc
+        return out
 
     def _irfft2(self, X):
         B, C = X.shape[:2]
