@@ -351,7 +351,7 @@ def run_serving(a):
         return Request(str(kind), N, C, th, f=f[i], phi=ph[i], n=7)
 
     # warm every shape once (graph capture, plans, kernel attributes) outside the measurement
-    srv = Server(max_batch=16, wf_workers=4).start()
+    srv = Server(max_batch=16).start()
     warm = [srv.submit(Request(k, N, C, th, f=pools[(N, C)][0][0], phi=pools[(N, C)][1][0], n=7))
             for N, th in SERVE_SIZES.items() for C in (1, 2) for k in ("lens", "delens")]
     warm += [srv.submit(Request("wf", N, C, th, problem=wf[(N, C)], n=7, wf_kwargs=wf_kw))

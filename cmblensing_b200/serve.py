@@ -84,7 +84,7 @@ def _bucket(b):
 class _LensSlot:
     """Static buffers, stream and captured graphs for batches of one (N, C, direction)."""
 
-    def __init__(self, dev, nside, ncomp, theta_pix, direction, cap, n, use_graphs):
+    def __init__(self, dev, nside, ncomp, theta_pix, direction, cap, n, use_graphs, priority=0):
         self.dev = dev
         self.nside, self.ncomp, self.direction, self.cap, self.n = nside, ncomp, direction, cap, n
         self.plan = engine.get_plan(nside, ncomp, theta_pix * ARCMIN, "f32", device=dev)
@@ -100,7 +100,7 @@ class _LensSlot:
         self.ws = torch.empty(max(self.plan.workspace_bytes(cap, True, n), 16), dtype=torch.uint8, device=dev)
         self.phi_ws = torch.empty(max(self.plan.phi_workspace_bytes(cap), 16), dtype=torch.uint8, device=dev)
         self.md = torch.empty(cap, dtype=torch.int32, device=dev)
-        self.stream = torch.cuda.Stream(dev)
+        self.stream = torch.cuda.Stream(dev, priority=priority)
         self.graphs = {}
         self.use_graphs = use_graphs
         self.busy = False
@@ -173,11 +173,17 @@ class _LensSlot:
 class Server:
     """Continuous-batching scheduler over the LenseFlow engine on one GPU."""
 
-    def __init__(self, hbm_budget=32 << 30, max_batch=16, use_graphs=True, wf_workers=4, wf_batch=8, device=None):
+    def __init__(self, hbm_budget=32 << 30, max_batch=16, use_graphs=True, wf_workers=2, wf_batch=8, device=None,
+                 lens_priority=-1):
         self.dev = torch.device("cuda", torch.cuda.current_device() if device is None else torch.device(device).index)
         self.budget = int(hbm_budget)
         self.max_batch = int(max_batch)
         self.use_graphs = use_graphs
+        # CUDA stream priority of the lens slots (lower = higher priority; 0 = the Wiener filters' level).
+        # Two Wiener-filter workers with the lens slots one level above them measured best for the
+        # mixed stream: 41 maps/s, lens p99 ~0.5 s, WF p50 ~4 s, against 33 maps/s, 1.2 s and 5.1 s
+        # with four workers at equal priority.
+        self.lens_priority = int(lens_priority)
         self.inbox = queue.Queue()
         self.pending = collections.defaultdict(collections.deque)  # group key -> requests
         self.slots = {}  # group key -> list of _LensSlot
@@ -236,7 +242,7 @@ class Server:
                 return s
         if len(self.slots[key]) < 2:  # two slots per shape: one can fill while the other runs
             N, C, th, direction = key
-            s = _LensSlot(self.dev, N, C, th, direction, self.max_batch, 7, self.use_graphs)
+            s = _LensSlot(self.dev, N, C, th, direction, self.max_batch, 7, self.use_graphs, self.lens_priority)
             self.slots[key].append(s)
             return s
         return None
