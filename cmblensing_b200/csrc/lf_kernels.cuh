@@ -115,6 +115,14 @@ __device__ __forceinline__ void load_twiddles(c2<T>* tw, const void* g, int tid)
   for (int i = tid; i < N; i += NT) tw[i] = src[i];
 }
 
+// Programmatic dependent launch.  A stage kernel lets the next kernel of the
+// stream launch once all its blocks are running (its blocks then fill SMs as
+// this grid drains), and waits for the previous kernel to complete, with its
+// memory visible, before touching any buffer the two share.  Without the
+// launch attribute both are no-ops.
+__device__ __forceinline__ void pdl_launch_dependents() { asm volatile("griddepcontrol.launch_dependents;" ::: "memory"); }
+__device__ __forceinline__ void pdl_wait() { asm volatile("griddepcontrol.wait;" ::: "memory"); }
+
 // shared-memory entries reserved for the column pass's twiddle table (rounded
 // up to an even count so that the tile after it stays 16-byte aligned); TWO:
 // the column table of the two-pass plan
@@ -137,8 +145,10 @@ __global__ void __launch_bounds__(NT, MINB) k_col(StageArgs a) {
   const int c0 = blockIdx.x * LINES;
   const long plane = blockIdx.y;
   static_assert(H % LINES == 0, "column tiles must cover the packed spectrum");
+  pdl_launch_dependents();
   if constexpr (TWO) load_twiddles<T, ctw_size(N), NT>(tw, a.twC, tid);
   else load_twiddles<T, ptw_size(N), NT>(tw, a.twP, tid);
+  pdl_wait();
   const c2<T>* in = reinterpret_cast<const c2<T>*>(a.s) + plane * (long)N * H + c0;
   c2<T>* out = reinterpret_cast<c2<T>*>(a.gx) + plane * (long)N * H + c0;
   // i KX / N^2 between the transforms; zero on KX's Nyquist row of the packed
@@ -186,7 +196,9 @@ __global__ void __launch_bounds__(NT, MINB) k_row(StageArgs a) {
   const int tid = threadIdx.x;
   const int r0 = blockIdx.x * LINES;
   const long map = blockIdx.y;
+  pdl_launch_dependents();
   load_twiddles<T, N, NT>(tw, a.twN, tid);
+  pdl_wait();
   const T* phi = reinterpret_cast<const T*>(a.phi) + map * 5 * P + (long)r0 * N;
   const T tnext = T(a.t_next);
   const T tcur = T(a.t_cur);
@@ -459,7 +471,9 @@ __global__ void __launch_bounds__(NT, MINB) k_row_pair(StageArgs a) {
   auto spec = [&](void* base, int c) {
     return reinterpret_cast<c2<T>*>(base) + (map * 2 + c) * half_plane + (long)r0 * H;
   };
+  pdl_launch_dependents();
   if (tid == 0) {
+    pdl_wait();  // the copies read what the previous kernel wrote
     mbar_init(mbar, 1);
     mbar_init(mbar + 1, 1);
     // the spectra first (the transforms wait for them): Gx_c and S_c rows, packed, into tile c
@@ -480,6 +494,7 @@ __global__ void __launch_bounds__(NT, MINB) k_row_pair(StageArgs a) {
   }
   load_twiddles<T, ptw_size(N), NT>(tw, a.twP, tid);  // pass table (fits the N entries reserved)
   static_assert(ptw_size(N) <= N, "pass table of the 8x8x8 plan");
+  pdl_wait();  // every thread, before its own global reads and writes
   constexpr int O8 = ptw_offset(N, R, R), O64 = ptw_offset(N, R, R * R);
   const T ky_scale = T(a.kbase / double(N));
   __syncthreads();  // barriers initialised before anyone waits on them
@@ -661,7 +676,9 @@ __global__ void __launch_bounds__(NT, MINB) k_row_pair_adj(StageArgs a) {
   auto spec = [&](void* base, int c) {
     return reinterpret_cast<c2<T>*>(base) + (map * 2 + c) * half_plane + (long)r0 * H;
   };
+  pdl_launch_dependents();
   if (tid == 0) {
+    pdl_wait();  // the copies read what the previous kernel wrote
     mbar_init(mbar, 1);
     mbar_init(mbar + 1, 1);
     // the spectra first: Gx_c and V_c rows, packed, into tile c
@@ -681,6 +698,7 @@ __global__ void __launch_bounds__(NT, MINB) k_row_pair_adj(StageArgs a) {
     }
   }
   load_twiddles<T, ptw_size(N), NT>(tw, a.twP, tid);
+  pdl_wait();  // every thread, before its own global reads and writes
   constexpr int O8 = ptw_offset(N, R, R), O64 = ptw_offset(N, R, R * R);
   const T ky_scale = T(a.kbase / double(N));
   __syncthreads();  // barriers initialised before anyone waits on them
