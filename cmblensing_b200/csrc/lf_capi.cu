@@ -189,11 +189,11 @@ cudaError_t launch_col(int planes, cudaStream_t st, const StageArgs& a) {
   if constexpr (std::is_same<T, float>::value && col2_plan(N)) {
     // 16-line tiles (128-byte row segments), 256 threads (one radix-32 butterfly each), 2 blocks per SM
     constexpr int NT2 = 256;
-    const size_t smem = sizeof(c2<T>) * (col_tw_entries(N, true) + LINES * N);
+    const size_t smem = sizeof(c2<T>) * (col_tw_entries(N, true) + LINES * N) + 16;  // + the table's mbarrier
     return launch_k<k_col<T, N, LINES, NT2, 2, true>>(LF_KIND_COL, grid, NT2, smem, st, a);
   } else {
     constexpr int NT = Geo<T>::nt(N);
-    const size_t smem = sizeof(c2<T>) * (col_tw_entries(N) + LINES * N);
+    const size_t smem = sizeof(c2<T>) * (col_tw_entries(N) + LINES * N) + 16;  // + the table's mbarrier
     return launch_k<k_col<T, N, LINES, NT, Geo<T>::minb(N)>>(LF_KIND_COL, grid, NT, smem, st, a);
   }
 }

@@ -244,6 +244,12 @@ __host__ __device__ constexpr int ptw_size(int L) {
 // previous passes.  ``tw`` holds NTAB entries.  ``pre(m, line, v)`` may
 // transform each input element as it is loaded (used to fold a spectral
 // multiplier into the first pass of a transform).
+// Called by fft_mul_ifft once its first pass (which reads no twiddles) has
+// been written to shared memory, before the second pass reads the table.
+struct NoHook {
+  __device__ __forceinline__ void operator()() const {}
+};
+
 struct NoPre {
   template <typename V> __device__ __forceinline__ V operator()(int, int, int, V v) const { return v; }
 };
@@ -397,9 +403,9 @@ __device__ __forceinline__ void sp_write(c2<T>* buf, c2<T> (&v)[SpGeom<L, R, LIN
 // twiddles ``twi``).  Shared memory sees one store and one load of the tile
 // per direction.  ``twf`` and ``twi`` are pass-table blocks: W^{r k} at
 // (r - 1) NS + k.
-template <typename T, int L, int R1, int R2, int LINES, int NT, class Src, class Mul, class Dst>
+template <typename T, int L, int R1, int R2, int LINES, int NT, class Src, class Mul, class Dst, class Hook = NoHook>
 __device__ __forceinline__ void fft_mul_ifft_2p(c2<T>* buf, const c2<T>* twf, const c2<T>* twi, int tid, Src src,
-                                                Mul mul, Dst dst) {
+                                                Mul mul, Dst dst, Hook hook = Hook()) {
   static_assert(R1 * R2 == L, "plan");
   auto smem = [=](int m, int line) { return buf[sw<T, LINES>(m, line)]; };
   c2<T> a[SpGeom<L, R1, LINES, NT>::PER][R1];
@@ -407,6 +413,7 @@ __device__ __forceinline__ void fft_mul_ifft_2p(c2<T>* buf, const c2<T>* twf, co
   sp_read<T, L, R1, 1, LINES, NT, false, L, true>(a, src, twf, tid);
   sp_write<T, L, R1, 1, LINES, NT>(buf, a, tid);
   __syncthreads();
+  hook();
   sp_read<T, L, R2, R1, LINES, NT, false, L, true>(b, smem, twf, tid);
   sp_apply<T, L, R2, R1, LINES, NT>(b, mul, tid);
 #pragma unroll
@@ -443,9 +450,9 @@ __host__ __device__ constexpr int ctw_size(int L) {
 // of 2 * (2 passes + 1).  ``mul(m, line, x)`` gets the spectrum at frequency m.
 // Plans: 32 = 8x4, 64 = 8x8, 128 = 8x16, 256 = 16x16, 512 = 8x8x8, 1024 = 16x8x8.
 // ``tw`` is the pass table of length L (ptw_size(L) entries).
-template <typename T, int L, int LINES, int NT, class Src, class Mul, class Dst>
+template <typename T, int L, int LINES, int NT, class Src, class Mul, class Dst, class Hook = NoHook>
 __device__ __forceinline__ void fft_mul_ifft(c2<T>* buf, const c2<T>* tw, int tid, Src src, Mul mul,
-                                             Dst dst) {
+                                             Dst dst, Hook hook = Hook()) {
   auto smem = [=](int m, int line) { return buf[sw<T, LINES>(m, line)]; };
   constexpr int R1 = plan_r1(L), R2 = plan_r2(L), R3 = plan_r3(L);
   // pass-table blocks (``tw`` is the pass table of length L); first passes read no twiddles
@@ -455,7 +462,7 @@ __device__ __forceinline__ void fft_mul_ifft(c2<T>* buf, const c2<T>* tw, int ti
   static_assert(OF2 >= 0 && OI2 >= 0 && (R3 == 1 || (OF3 >= 0 && OI3 >= 0)), "pass table block missing");
   static_assert(L == 32 || L == 64 || L == 128 || L == 256 || L == 512 || L == 1024, "unsupported length");
   if constexpr (R3 == 1) {
-    fft_mul_ifft_2p<T, L, R1, R2, LINES, NT>(buf, tw + OF2, tw + OI2, tid, src, mul, dst);
+    fft_mul_ifft_2p<T, L, R1, R2, LINES, NT>(buf, tw + OF2, tw + OI2, tid, src, mul, dst, hook);
   } else {
     static_assert(R1 * R2 * R3 == L, "plan");
     c2<T> a[SpGeom<L, R1, LINES, NT>::PER][R1];
@@ -464,6 +471,7 @@ __device__ __forceinline__ void fft_mul_ifft(c2<T>* buf, const c2<T>* tw, int ti
     sp_read<T, L, R1, 1, LINES, NT, false, L, true>(a, src, tw, tid);
     sp_write<T, L, R1, 1, LINES, NT>(buf, a, tid);
     __syncthreads();
+    hook();
     sp_read<T, L, R2, R1, LINES, NT, false, L, true>(b, smem, tw + OF2, tid);
     __syncthreads();
     sp_write<T, L, R2, R1, LINES, NT>(buf, b, tid);

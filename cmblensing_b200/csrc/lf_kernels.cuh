@@ -130,6 +130,54 @@ __host__ __device__ constexpr int col_tw_entries(int n, bool two = false) {
   return ((two ? ctw_size(n) : ptw_size(n)) + 1) & ~1;
 }
 
+// ============================================ bulk copies and bounded waits
+// Set (never cleared by the kernels) when a block gave up waiting for its
+// bulk copies; the host reads it with lf_wait_timeouts().
+__device__ int g_lf_wait_timeouts;
+
+__device__ __forceinline__ uint32_t smem_addr(const void* p) {
+  return static_cast<uint32_t>(__cvta_generic_to_shared(p));
+}
+
+__device__ __forceinline__ void mbar_init(uint64_t* mbar, int count) {
+  asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(smem_addr(mbar)), "r"(count) : "memory");
+  // make the initialised barrier visible to the bulk-copy (async) proxy
+  asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+}
+
+__device__ __forceinline__ void mbar_expect_tx(uint64_t* mbar, uint32_t bytes) {
+  asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(smem_addr(mbar)), "r"(bytes)
+               : "memory");
+}
+
+// One contiguous global -> shared copy of ``bytes`` (16-byte aligned, multiple of 16).
+__device__ __forceinline__ void bulk_g2s(void* dst, const void* src, uint32_t bytes, uint64_t* mbar) {
+  asm volatile(
+      "cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];" ::"r"(
+          smem_addr(dst)),
+      "l"(src), "r"(bytes), "r"(smem_addr(mbar))
+      : "memory");
+}
+
+// Wait for phase ``parity`` of the barrier, giving up after ``tries`` polls;
+// each poll suspends for at most about 1 microsecond (the explicit time hint),
+// so a wait is bounded by roughly tries microseconds.
+__device__ __forceinline__ bool mbar_wait(uint64_t* mbar, uint32_t parity, int tries) {
+  const uint32_t addr = smem_addr(mbar);
+  for (int i = 0; i < tries; ++i) {
+    uint32_t done;
+    asm volatile(
+        "{\n .reg .pred p;\n mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2, %3;\n selp.u32 %0, 1, 0, p;\n}"
+        : "=r"(done)
+        : "r"(addr), "r"(parity), "r"(1000u)
+        : "memory");
+    if (done) return true;
+  }
+  return false;
+}
+
+constexpr int kWaitTries = 1 << 20;  // about one second
+
 // ======================================================== column pass
 // Gx = IFFT_col( (i KX / N^2) * FFT_col(S) ) on tiles of LINES columns.
 // grid: x = column tile (N/2/LINES), y = plane.  TWO: the plan N = 16 x 32
@@ -141,14 +189,29 @@ __global__ void __launch_bounds__(NT, MINB) k_col(StageArgs a) {
   extern __shared__ __align__(16) unsigned char smem_raw[];
   c2<T>* tw = reinterpret_cast<c2<T>*>(smem_raw);  // pass table or column table
   c2<T>* buf = tw + col_tw_entries(N, TWO);
+  uint64_t* mbar = reinterpret_cast<uint64_t*>(buf + LINES * N);  // 16 bytes reserved after the tile
   const int tid = threadIdx.x;
   const int c0 = blockIdx.x * LINES;
   const long plane = blockIdx.y;
   static_assert(H % LINES == 0, "column tiles must cover the packed spectrum");
+  constexpr int NTW = TWO ? ctw_size(N) : ptw_size(N);
+  static_assert(NTW * sizeof(c2<T>) % 16 == 0, "twiddle table: one bulk copy");
   pdl_launch_dependents();
-  if constexpr (TWO) load_twiddles<T, ctw_size(N), NT>(tw, a.twC, tid);
-  else load_twiddles<T, ptw_size(N), NT>(tw, a.twP, tid);
+  if (tid == 0) {  // the table by one bulk copy; the first pass, which reads none of it, runs meanwhile
+    mbar_init(mbar, 1);
+    mbar_expect_tx(mbar, uint32_t(NTW * sizeof(c2<T>)));
+    bulk_g2s(tw, TWO ? a.twC : a.twP, NTW * sizeof(c2<T>), mbar);
+  }
   pdl_wait();
+  // after the first pass's barrier (which also orders the barrier's init before the waits)
+  auto wait_table = [=]() {
+    if (!mbar_wait(mbar, 0, kWaitTries)) {
+      // the table never arrived: record it (this launch's results are then
+      // invalid), let the copy drain, and go on to the remaining barriers
+      atomicExch(&g_lf_wait_timeouts, 1);
+      mbar_wait(mbar, 0, kWaitTries);
+    }
+  };
   const c2<T>* in = reinterpret_cast<const c2<T>*>(a.s) + plane * (long)N * H + c0;
   c2<T>* out = reinterpret_cast<c2<T>*>(a.gx) + plane * (long)N * H + c0;
   // i KX / N^2 between the transforms; zero on KX's Nyquist row of the packed
@@ -163,9 +226,10 @@ __global__ void __launch_bounds__(NT, MINB) k_col(StageArgs a) {
   auto src = [=](int m, int line) { return in[m * H + line]; };
   auto dst = [=](int m, int line, c2<T> x) { out[m * H + line] = x; };
   if constexpr (TWO)
-    fft_mul_ifft_2p<T, N, col2_r1(N), col2_r2(N), LINES, NT>(buf, tw, tw + ctw_inv_offset(N), tid, src, kx_mul, dst);
+    fft_mul_ifft_2p<T, N, col2_r1(N), col2_r2(N), LINES, NT>(buf, tw, tw + ctw_inv_offset(N), tid, src, kx_mul, dst,
+                                                           wait_table);
   else
-    fft_mul_ifft<T, N, LINES, NT>(buf, tw, tid, src, kx_mul, dst);
+    fft_mul_ifft<T, N, LINES, NT>(buf, tw, tid, src, kx_mul, dst, wait_table);
 }
 
 // ========================================================= row pass
@@ -375,54 +439,6 @@ __global__ void __launch_bounds__(NT, MINB) k_row(StageArgs a) {
   }
 }
 
-// ============================================ bulk copies and bounded waits
-// Set (never cleared by the kernels) when a block gave up waiting for its
-// bulk copies; the host reads it with lf_wait_timeouts().
-__device__ int g_lf_wait_timeouts;
-
-__device__ __forceinline__ uint32_t smem_addr(const void* p) {
-  return static_cast<uint32_t>(__cvta_generic_to_shared(p));
-}
-
-__device__ __forceinline__ void mbar_init(uint64_t* mbar, int count) {
-  asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(smem_addr(mbar)), "r"(count) : "memory");
-  // make the initialised barrier visible to the bulk-copy (async) proxy
-  asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
-}
-
-__device__ __forceinline__ void mbar_expect_tx(uint64_t* mbar, uint32_t bytes) {
-  asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(smem_addr(mbar)), "r"(bytes)
-               : "memory");
-}
-
-// One contiguous global -> shared copy of ``bytes`` (16-byte aligned, multiple of 16).
-__device__ __forceinline__ void bulk_g2s(void* dst, const void* src, uint32_t bytes, uint64_t* mbar) {
-  asm volatile(
-      "cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];" ::"r"(
-          smem_addr(dst)),
-      "l"(src), "r"(bytes), "r"(smem_addr(mbar))
-      : "memory");
-}
-
-// Wait for phase ``parity`` of the barrier, giving up after ``tries`` polls;
-// each poll suspends for at most about 1 microsecond (the explicit time hint),
-// so a wait is bounded by roughly tries microseconds.
-__device__ __forceinline__ bool mbar_wait(uint64_t* mbar, uint32_t parity, int tries) {
-  const uint32_t addr = smem_addr(mbar);
-  for (int i = 0; i < tries; ++i) {
-    uint32_t done;
-    asm volatile(
-        "{\n .reg .pred p;\n mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2, %3;\n selp.u32 %0, 1, 0, p;\n}"
-        : "=r"(done)
-        : "r"(addr), "r"(parity), "r"(1000u)
-        : "memory");
-    if (done) return true;
-  }
-  return false;
-}
-
-constexpr int kWaitTries = 1 << 20;  // about one second
-
 // ============================================ row pass, component pairs
 // Standard RHS for two components (Q, U) with the p planes, N = 512, FP32.
 // The general row pass inverse-transforms four packed half spectra per row
@@ -471,13 +487,16 @@ __global__ void __launch_bounds__(NT, MINB) k_row_pair(StageArgs a) {
   auto spec = [&](void* base, int c) {
     return reinterpret_cast<c2<T>*>(base) + (map * 2 + c) * half_plane + (long)r0 * H;
   };
+  static_assert(ptw_size(N) <= N && ptw_size(N) * sizeof(c2<T>) % 16 == 0, "pass table: one bulk copy");
   pdl_launch_dependents();
   if (tid == 0) {
-    pdl_wait();  // the copies read what the previous kernel wrote
     mbar_init(mbar, 1);
     mbar_init(mbar + 1, 1);
-    // the spectra first (the transforms wait for them): Gx_c and S_c rows, packed, into tile c
-    mbar_expect_tx(mbar + 1, uint32_t(4 * LINES * H * sizeof(c2<T>)));
+    // the pass table and the spectra first (the transforms wait for them)
+    mbar_expect_tx(mbar + 1, uint32_t(ptw_size(N) * sizeof(c2<T>) + 4 * LINES * H * sizeof(c2<T>)));
+    bulk_g2s(tw, a.twP, ptw_size(N) * sizeof(c2<T>), mbar + 1);
+    pdl_wait();  // the other copies read what the previous kernel wrote
+    // Gx_c and S_c rows, packed, into tile c
     for (int c = 0; c < 2; ++c) {
       bulk_g2s(buf + c * TILE, spec(a.gx, c), LINES * H * sizeof(c2<T>), mbar + 1);
       bulk_g2s(buf + c * TILE + LINES * H, spec(a.s, c), LINES * H * sizeof(c2<T>), mbar + 1);
@@ -492,16 +511,14 @@ __global__ void __launch_bounds__(NT, MINB) k_row_pair(StageArgs a) {
       bulk_g2s(stg + (4 + c) * RB, pp + c * P, RB * sizeof(T), mbar);
     }
   }
-  load_twiddles<T, ptw_size(N), NT>(tw, a.twP, tid);  // pass table (fits the N entries reserved)
-  static_assert(ptw_size(N) <= N, "pass table of the 8x8x8 plan");
   pdl_wait();  // every thread, before its own global reads and writes
   constexpr int O8 = ptw_offset(N, R, R), O64 = ptw_offset(N, R, R * R);
   const T ky_scale = T(a.kbase / double(N));
   __syncthreads();  // barriers initialised before anyone waits on them
   if (!mbar_wait(mbar + 1, 0, kWaitTries)) {
-    // the spectra never arrived: record it (this launch's results are then
-    // invalid), let the copies drain, and go on so that every thread meets
-    // every barrier below
+    // the pass table and spectra never arrived: record it (this launch's
+    // results are then invalid), let the copies drain, and go on so that
+    // every thread meets every barrier below
     atomicExch(&g_lf_wait_timeouts, 1);
     mbar_wait(mbar + 1, 0, kWaitTries);
   }
@@ -676,13 +693,16 @@ __global__ void __launch_bounds__(NT, MINB) k_row_pair_adj(StageArgs a) {
   auto spec = [&](void* base, int c) {
     return reinterpret_cast<c2<T>*>(base) + (map * 2 + c) * half_plane + (long)r0 * H;
   };
+  static_assert(ptw_size(N) <= N && ptw_size(N) * sizeof(c2<T>) % 16 == 0, "pass table: one bulk copy");
   pdl_launch_dependents();
   if (tid == 0) {
-    pdl_wait();  // the copies read what the previous kernel wrote
     mbar_init(mbar, 1);
     mbar_init(mbar + 1, 1);
-    // the spectra first: Gx_c and V_c rows, packed, into tile c
-    mbar_expect_tx(mbar + 1, uint32_t(4 * LINES * H * sizeof(c2<T>)));
+    // the pass table and the spectra first
+    mbar_expect_tx(mbar + 1, uint32_t(ptw_size(N) * sizeof(c2<T>) + 4 * LINES * H * sizeof(c2<T>)));
+    bulk_g2s(tw, a.twP, ptw_size(N) * sizeof(c2<T>), mbar + 1);
+    pdl_wait();  // the other copies read what the previous kernel wrote
+    // Gx_c and V_c rows, packed, into tile c
     for (int c = 0; c < 2; ++c) {
       bulk_g2s(buf + c * TILE, spec(a.gx, c), LINES * H * sizeof(c2<T>), mbar + 1);
       bulk_g2s(buf + c * TILE + LINES * H, spec(a.v, c), LINES * H * sizeof(c2<T>), mbar + 1);
@@ -697,15 +717,14 @@ __global__ void __launch_bounds__(NT, MINB) k_row_pair_adj(StageArgs a) {
       bulk_g2s(stg + (4 + c) * RB, pp + c * P, RB * sizeof(T), mbar);
     }
   }
-  load_twiddles<T, ptw_size(N), NT>(tw, a.twP, tid);
   pdl_wait();  // every thread, before its own global reads and writes
   constexpr int O8 = ptw_offset(N, R, R), O64 = ptw_offset(N, R, R * R);
   const T ky_scale = T(a.kbase / double(N));
   __syncthreads();  // barriers initialised before anyone waits on them
   if (!mbar_wait(mbar + 1, 0, kWaitTries)) {
-    // the spectra never arrived: record it (this launch's results are then
-    // invalid), let the copies drain, and go on so that every thread meets
-    // every barrier below
+    // the pass table and spectra never arrived: record it (this launch's
+    // results are then invalid), let the copies drain, and go on so that
+    // every thread meets every barrier below
     atomicExch(&g_lf_wait_timeouts, 1);
     mbar_wait(mbar + 1, 0, kWaitTries);
   }
