@@ -204,7 +204,7 @@ cudaError_t run_lens_pp(const StageArgs& base, int B, int nsteps, double t0, dou
   constexpr int RNT = Geo<T>::row_nt(N);
   constexpr int RMB = Geo<T>::row_minb(N, C);
   constexpr int H = N / 2;
-  const size_t smem_row = sizeof(c2<T>) * (N + 2 * C * RL * H);
+  const size_t smem_row = sizeof(c2<T>) * (N + 2 * C * RL * H) + 16;  // + the table's mbarrier
   const dim3 grow(N / RL, B);
   StageArgs a = base;
   cudaError_t e;
@@ -432,7 +432,7 @@ cudaError_t run_vjp_n(const StageArgs& af0, const StageArgs& ad0, double* dacc, 
   constexpr int RNT = Geo<T>::row_nt(N);
   constexpr int RMB = Geo<T>::row_minb(N, C);
   constexpr int H = N / 2;
-  const size_t smem_row = sizeof(c2<T>) * (N + 2 * C * RL * H);
+  const size_t smem_row = sizeof(c2<T>) * (N + 2 * C * RL * H) + 16;  // + the table's mbarrier
   const dim3 grow(N / RL, B);
   const long P = (long)N * N;
   const int gacc = (int)std::min<long>(((long)B * P + 255) / 256, 4096);

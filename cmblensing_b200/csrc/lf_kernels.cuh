@@ -260,9 +260,24 @@ __global__ void __launch_bounds__(NT, MINB) k_row(StageArgs a) {
   const int tid = threadIdx.x;
   const int r0 = blockIdx.x * LINES;
   const long map = blockIdx.y;
+  uint64_t* mbar = reinterpret_cast<uint64_t*>(buf + 2 * C * TILE);  // 16 bytes reserved after the tiles
+  static_assert(N * sizeof(c2<T>) % 16 == 0, "twiddle table: one bulk copy");
   pdl_launch_dependents();
-  load_twiddles<T, N, NT>(tw, a.twN, tid);
+  if (tid == 0) {  // the table by one bulk copy while the rows load
+    mbar_init(mbar, 1);
+    mbar_expect_tx(mbar, uint32_t(N * sizeof(c2<T>)));
+    bulk_g2s(tw, a.twN, N * sizeof(c2<T>), mbar);
+  }
   pdl_wait();
+  // after the barrier that follows the row loads (it also orders the init before the waits)
+  auto wait_table = [=]() {
+    if (!mbar_wait(mbar, 0, kWaitTries)) {
+      // the table never arrived: record it (this launch's results are then
+      // invalid), let the copy drain, and go on to the remaining barriers
+      atomicExch(&g_lf_wait_timeouts, 1);
+      mbar_wait(mbar, 0, kWaitTries);
+    }
+  };
   const T* phi = reinterpret_cast<const T*>(a.phi) + map * 5 * P + (long)r0 * N;
   const T tnext = T(a.t_next);
   const T tcur = T(a.t_cur);
@@ -284,6 +299,7 @@ __global__ void __launch_bounds__(NT, MINB) k_row(StageArgs a) {
       load_rows<T, c2<T>, H, LINES, NT>(buf + (C + c) * TILE, spec(ADJ ? a.v : a.s, c), H, tid);
     }
     __syncthreads();
+    wait_table();
     // d_y in the row spectrum: i KY / N, folded into the pre-pass of the
     // inverse real transform (KY's DC and Nyquist bins contribute nothing
     // after it, so the (X0, XH) slot of a d_y spectrum is zero).
@@ -311,6 +327,7 @@ __global__ void __launch_bounds__(NT, MINB) k_row(StageArgs a) {
       buf[c * TILE + sw<T, LINES>(m, row)] = load_io<T>(a.f_in, a.in_f64, fo);
     }
     __syncthreads();
+    wait_table();
   }
 
   // ---------------------------------------------------- pointwise epilogue
