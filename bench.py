@@ -267,7 +267,7 @@ def col_bytes_per_lens(C, n, P):
 # launch are stage1_bytes_per_map(C) N^2; the reads equal them, the writes
 # fall short by what is still in L2 when the launch ends.
 NCU_STAGE1_TRAFFIC_PER_MAP = {
-    ("k_row_pair", 512, 2): (134.27e6 + 30.59e6) / 16,
+    ("k_row_pair", 512, 2): (134.28e6 + 32.36e6) / 16,
     ("k_row_pair_adj", 512, 2): (134.27e6 + 51.79e6) / 16,
 }
 
