@@ -309,8 +309,8 @@ cudaError_t run_phi_n(const void* phi, int basis, int B, TO* planes, int* min_de
   constexpr int H = N / 2;
   double2* spec = reinterpret_cast<double2*>(ws);            // [B][N][H+1]
   double2* packed = spec + (size_t)B * N * (H + 1);          // [B][5][N][H]
-  const size_t smem_row = sizeof(double2) * (N + LINES * H);
-  const size_t smem_col = sizeof(double2) * (N + LINES * N);
+  const size_t smem_row = sizeof(double2) * (N + LINES * H) + 16;  // + the table's mbarrier
+  const size_t smem_col = sizeof(double2) * (N + LINES * N) + 16;  // + the table's mbarrier
   const int ctiles = (H + 1 + LINES - 1) / LINES;
   cudaError_t e;
   if (basis == LF_PHI_MAP) {
@@ -354,8 +354,8 @@ cudaError_t run_rfft2_n(const void* maps, int in_f64, int B, double2* spec, cons
   constexpr int LINES = 8;
   constexpr int NT = Geo<double>::nt(N);
   constexpr int H = N / 2;
-  const size_t smem_row = sizeof(double2) * (N + LINES * H);
-  const size_t smem_col = sizeof(double2) * (N + LINES * N);
+  const size_t smem_row = sizeof(double2) * (N + LINES * H) + 16;  // + the table's mbarrier
+  const size_t smem_col = sizeof(double2) * (N + LINES * N) + 16;  // + the table's mbarrier
   const int ctiles = (H + 1 + LINES - 1) / LINES;
   cudaError_t e;
   if (in_f64)
@@ -374,8 +374,8 @@ cudaError_t run_irfft2_n(const double2* spec, int B, void* maps, int out_f64, do
   constexpr int LINES = 8;
   constexpr int NT = Geo<double>::nt(N);
   constexpr int H = N / 2;
-  const size_t smem_row = sizeof(double2) * (N + LINES * H);
-  const size_t smem_col = sizeof(double2) * (N + LINES * N);
+  const size_t smem_row = sizeof(double2) * (N + LINES * H) + 16;  // + the table's mbarrier
+  const size_t smem_col = sizeof(double2) * (N + LINES * N) + 16;  // + the table's mbarrier
   const int ctiles = (H + 1 + LINES - 1) / LINES;
   cudaError_t e = launch<k_spec_cols_inv<N, LINES, NT>>(dim3(ctiles, B), NT, smem_col, st, spec, packed, tw64);
   if (e != cudaSuccess) return e;

@@ -901,6 +901,27 @@ __global__ void __launch_bounds__(256) k_p_planes(const T* __restrict__ planes, 
 }
 
 // ================================================ phi precompute (FP64)
+// Each block's float64 twiddle table arrives by one bulk copy (thread 0, on
+// an mbarrier placed after the block's tile) while the block loads its data;
+// table_wait follows a barrier and precedes the first pass that reads it.
+template <int NTAB>
+__device__ __forceinline__ void table_copy(double2* tw, const double2* src, uint64_t* mbar, int tid) {
+  static_assert(NTAB * sizeof(double2) % 16 == 0, "twiddle table: one bulk copy");
+  if (tid == 0) {
+    mbar_init(mbar, 1);
+    mbar_expect_tx(mbar, uint32_t(NTAB * sizeof(double2)));
+    bulk_g2s(tw, src, NTAB * sizeof(double2), mbar);
+  }
+}
+
+__device__ __forceinline__ void table_wait(uint64_t* mbar) {
+  if (!mbar_wait(mbar, 0, kWaitTries)) {
+    // the table never arrived: record it (this launch's results are then
+    // invalid), let the copy drain, and go on to the remaining barriers
+    atomicExch(&g_lf_wait_timeouts, 1);
+    mbar_wait(mbar, 0, kWaitTries);
+  }
+}
 // rfft along rows of a real map (N x N double) into the unpacked
 // (N x (N/2+1)) complex layout of rfft2.   grid: x = row tile, y = map.
 template <int N, int LINES, int NT, typename TI = double>
@@ -913,10 +934,12 @@ __global__ void __launch_bounds__(NT) k_phi_rows_r2c(const TI* __restrict__ phi,
   const int tid = threadIdx.x;
   const int r0 = blockIdx.x * LINES;
   const long map = blockIdx.y;
-  load_twiddles<double, N, NT>(tw, twN, tid);
+  uint64_t* mbar = reinterpret_cast<uint64_t*>(buf + LINES * H);
+  table_copy<N>(tw, twN, mbar, tid);
   const c2<TI>* src = reinterpret_cast<const c2<TI>*>(phi + map * (long)N * N + (long)r0 * N);
   load_rows<double, c2<TI>, H, LINES, NT>(buf, src, H, tid);
   __syncthreads();
+  table_wait(mbar);
   fft_tiles<double, H, LINES, 1, NT, false, N>(buf, tw, tid);
   r2c_post<double, H, LINES, 1, NT>(buf, tw, tid);
   double2* dst = out + map * (long)N * (H + 1) + (long)r0 * (H + 1);
@@ -944,9 +967,11 @@ __global__ void __launch_bounds__(NT) k_phi_cols_fwd(double2* __restrict__ arr, 
   const int tid = threadIdx.x;
   const int c0 = blockIdx.x * LINES;
   double2* a = arr + blockIdx.y * (long)N * (H + 1);
-  load_twiddles<double, N, NT>(tw, twN, tid);
+  uint64_t* mbar = reinterpret_cast<uint64_t*>(buf + LINES * N);
+  table_copy<N>(tw, twN, mbar, tid);
   load_cols<double, N, LINES, NT>(buf, a, H + 1, c0, H + 1, tid);
   __syncthreads();
+  table_wait(mbar);
   fft_tiles<double, N, LINES, 1, NT, false, N>(buf, tw, tid);
   store_cols<double, N, LINES, NT>(a, H + 1, c0, H + 1, buf, tid);
 }
@@ -971,7 +996,8 @@ __global__ void __launch_bounds__(NT) k_phi_cols_deriv(const double2* __restrict
   const int c0 = blockIdx.x * LINES;
   const long map = blockIdx.y;
   const double2* a = spec + map * (long)N * (H + 1);
-  load_twiddles<double, N, NT>(tw, twN, tid);
+  uint64_t* mbar = reinterpret_cast<uint64_t*>(buf + LINES * N);
+  table_copy<N>(tw, twN, mbar, tid);
   const double scale = 1.0 / (double(N) * double(N));
   // (G, output j, KY power): KY power 0 = G itself, 1 = i KY G, 2 = -KY^2 G
   constexpr int kOut[3][2][2] = {{{1, 1}, {4, 2}}, {{0, 0}, {3, 1}}, {{2, 0}, {-1, 0}}};
@@ -990,6 +1016,7 @@ __global__ void __launch_bounds__(NT) k_phi_cols_deriv(const double2* __restrict
       buf[sw<double, LINES>(m, line)] = r;
     }
     __syncthreads();
+    if (g == 0) table_wait(mbar);
     fft_tiles<double, N, LINES, 1, NT, true, N>(buf, tw, tid);
     for (int o = 0; o < 2; ++o) {
       const int j = kOut[g][o][0], pw = kOut[g][o][1];
@@ -1026,9 +1053,11 @@ __global__ void __launch_bounds__(NT) k_phi_rows_c2r(const double2* __restrict__
   const int tid = threadIdx.x;
   const int r0 = blockIdx.x * LINES;
   const long pl = blockIdx.y;
-  load_twiddles<double, N, NT>(tw, twN, tid);
+  uint64_t* mbar = reinterpret_cast<uint64_t*>(buf + LINES * H);
+  table_copy<N>(tw, twN, mbar, tid);
   load_rows<double, double2, H, LINES, NT>(buf, packed + pl * (long)N * H + (long)r0 * H, H, tid);
   __syncthreads();
+  table_wait(mbar);
   c2r_pre<double, H, LINES, 1, NT>(buf, tw, tid);
   fft_tiles<double, H, LINES, 1, NT, true, N>(buf, tw, tid);
   using O2 = c2<TO>;
@@ -1137,9 +1166,11 @@ __global__ void __launch_bounds__(NT) k_spec_cols_inv(const double2* __restrict_
   const int tid = threadIdx.x;
   const int c0 = blockIdx.x * LINES;
   const long map = blockIdx.y;
-  load_twiddles<double, N, NT>(tw, twN, tid);
+  uint64_t* mbar = reinterpret_cast<uint64_t*>(buf + LINES * N);
+  table_copy<N>(tw, twN, mbar, tid);
   load_cols<double, N, LINES, NT>(buf, spec + map * (long)N * (H + 1), H + 1, c0, H + 1, tid);
   __syncthreads();
+  table_wait(mbar);
   const double scale = 1.0 / (double(N) * double(N));
   for (int idx = tid; idx < N * LINES; idx += NT) {
     const int m = idx / LINES, line = idx % LINES;
