@@ -38,6 +38,9 @@ SIGNATURES = {
     "lf_workspace_bytes": (_sz, [_vp, _i, _i]),
     "lf_workspace_bytes_n": (_sz, [_vp, _i, _i, _i]),
     "lf_wait_timeouts": (_i, [ctypes.POINTER(ctypes.c_int), _i]),
+    "lf_timeout_status": (_i, []),
+    "lf_stream_check": (_i, [_vp]),
+    "lf_set_wait_polls": (_i, [_i]),
     "lf_phi_planes_bytes": (_sz, [_vp, _i]),
     "lf_phi_workspace_bytes": (_sz, [_vp, _i]),
     "lf_phi_precompute": (_i, [_vp, _vp, _i, _i, _vp, _vp, _vp, _sz, _vp]),
@@ -49,6 +52,8 @@ SIGNATURES = {
     "lf_irfft2": (_i, [_vp, _vp, _i, _vp, _i, _vp, _sz, _vp]),
     "lf_vjp_workspace_bytes": (_sz, [_vp, _i]),
     "lf_lense_flow_vjp": (_i, [_vp, _vp, _vp, _i, _vp, _i, _i, _i, _vp, _vp, _vp, _i, _vp, _sz, _vp]),
+    "lf_vjp_ckpt_workspace_bytes": (_sz, [_vp, _i, _i]),
+    "lf_lense_flow_vjp_ckpt": (_i, [_vp, _vp, _vp, _i, _vp, _i, _i, _i, _vp, _vp, _vp, _i, _vp, _sz, _vp]),
     "lf_lense_flow_noalloc": (_i, [_i, _i, ctypes.c_double, _vp, _i, _vp, _i, _vp, _i, _i, _i, _i, _vp]),
     "lf_profile_enable": (_i, [_vp, _i]),
     "lf_profile_reset": (_i, [_vp]),

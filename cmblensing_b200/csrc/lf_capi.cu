@@ -3,6 +3,7 @@
 #include <stdint.h>
 
 #include <algorithm>
+#include <atomic>
 #include <cmath>
 #include <cstring>
 #include <mutex>
@@ -119,16 +120,61 @@ template <> struct Geo<double> {
 };
 
 // Opt in to > 48 KB of dynamic shared memory once per kernel and device.
+// Host threads may launch concurrently (a plan per thread, the allocation-free
+// entry point): the per-device high-water mark is an atomic, and a racing
+// thread at worst sets the same attribute twice.
 template <auto Kernel>
 cudaError_t ensure_smem(size_t smem) {
-  static size_t done[64] = {0};
+  static std::atomic<size_t> done[64];
   int dev = 0;
   cudaGetDevice(&dev);
   if (dev < 0 || dev >= 64) return cudaErrorInvalidDevice;
-  if (done[dev] >= smem) return cudaSuccess;
+  if (done[dev].load(std::memory_order_relaxed) >= smem) return cudaSuccess;
   cudaError_t e = cudaFuncSetAttribute(Kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
-  if (e == cudaSuccess) done[dev] = smem;
+  if (e == cudaSuccess) {
+    size_t cur = done[dev].load(std::memory_order_relaxed);
+    while (cur < smem && !done[dev].compare_exchange_weak(cur, smem, std::memory_order_relaxed)) {
+    }
+  }
   return e;
+}
+
+// ------------------------------------------------------ wait timeouts
+// One mapped pinned host word per process; its device address goes to
+// g_lf_timeout_host on every device that creates a plan.  Kernels whose
+// bounded wait runs out set it; entry points read it (no synchronisation)
+// and return LF_ERR_TIMEOUT while it is set.
+std::mutex g_flag_mu;
+std::atomic<int*> g_host_flag{nullptr};
+bool g_flag_on_device[64] = {false};
+
+cudaError_t ensure_timeout_flag() {
+  int dev = 0;
+  cudaError_t e = cudaGetDevice(&dev);
+  if (e != cudaSuccess) return e;
+  if (dev < 0 || dev >= 64) return cudaErrorInvalidDevice;
+  std::lock_guard<std::mutex> lock(g_flag_mu);
+  if (!g_host_flag.load()) {
+    void* h = nullptr;
+    e = cudaHostAlloc(&h, sizeof(int), cudaHostAllocMapped | cudaHostAllocPortable);
+    if (e != cudaSuccess) return e;
+    *static_cast<volatile int*>(h) = 0;
+    g_host_flag.store(static_cast<int*>(h));
+  }
+  if (!g_flag_on_device[dev]) {
+    int* d = nullptr;
+    e = cudaHostGetDevicePointer(reinterpret_cast<void**>(&d), g_host_flag.load(), 0);
+    if (e == cudaSuccess) e = cudaMemcpyToSymbol(g_lf_timeout_host, &d, sizeof(d));
+    if (e != cudaSuccess) return e;
+    g_flag_on_device[dev] = true;
+  }
+  return cudaSuccess;
+}
+
+// True once a kernel has recorded a timeout that no lf_wait_timeouts reset has cleared.
+bool timeout_recorded() {
+  const int* h = g_host_flag.load(std::memory_order_acquire);
+  return h && *reinterpret_cast<const volatile int*>(h) != 0;
 }
 
 thread_local Prof* g_prof = nullptr;  // profiler of the plan whose call is running on this thread
@@ -494,6 +540,177 @@ cudaError_t run_vjp(int N, int C, const StageArgs& af, const StageArgs& ad, doub
   }
 }
 
+// --------------------------------------------- checkpointed exact VJP
+// Workspace of lf_lense_flow_vjp_ckpt, in order: the n step checkpoints, the
+// forward state (y0, acc, S, Gx), the four stage gradients (d_x u_s, d_y u_s),
+// the adjoint state (y0, acc, U, V, Gx), the saved adjoint stage input, an
+// output sink, the delta-phi accumulators and the spectra of the final combine.
+struct CkptLayout {
+  size_t ckpt, f_sys, grads, d_sys, dsave, sink, dacc, spec, dphi_f, total;
+  CkptLayout(int N, int C, int B, int n, size_t el) {
+    const size_t bcp = (size_t)B * C * N * N, bp = (size_t)B * N * N, half = (size_t)B * N * (N / 2 + 1);
+    ckpt = (size_t)n * el * bcp;
+    f_sys = 4 * el * bcp;
+    grads = 4 * 2 * el * bcp;
+    d_sys = 5 * el * bcp;
+    dsave = el * bcp;
+    sink = 8 * bcp;
+    dacc = 5 * 8 * bp;
+    spec = 5 * 16 * half;
+    dphi_f = 16 * half;
+    total = ckpt + f_sys + grads + d_sys + dsave + sink + dacc + spec + dphi_f;
+  }
+};
+
+// The exact transpose of the discrete forward RK4 (lense_flow.py:336-352 with
+// util.py:184-199).  The forward integration stores y_i at the start of every
+// step.  Backwards, step i is recomputed from y_i with its four stage
+// inputs' gradients saved (d_x u_s, d_y u_s), and one RK4 step of the
+// adjoint RHS carries the cotangent from t_{i+1} to t_i: for a linear RHS the
+// transpose of an RK4 step is an RK4 step of the transposed RHS with the
+// stages in reverse order (forward stage s pairs with adjoint stage 5 - s at
+// the same time).  The stage cotangents are k_bar_s = (h/6) w_s v_{5-s},
+// w = {1, 2, 2, 1}, with v_j the adjoint stage inputs, so
+// p_bar(t_s) += k_bar_s . grad u_s, and the chain rule through
+// p = M(t)^-1 grad(phi) is the same per-stage delta-phi rate as the
+// reference's reverse ODE (get_delta_phi_tqu_roc, lense_flow.py:195-252) --
+// evaluated on the forward stage inputs u_s instead of a field re-integrated
+// backwards from Lf.  The result is the gradient of the discrete map, free of
+// the reference scheme's O(h^4) gap.
+template <typename T, int N, int C>
+cudaError_t run_vjp_ckpt_n(const StageArgs& af0, const StageArgs& ad0, char* ckpt, char* grads, void* sink, double* dacc,
+                           int B, int nsteps, double t0, double t1, cudaStream_t st) {
+  constexpr int RL = Geo<T>::ROW_LINES;
+  constexpr int RNT = Geo<T>::row_nt(N);
+  constexpr int RMB = Geo<T>::row_minb(N, C);
+  constexpr int H = N / 2;
+  const size_t smem_row = sizeof(c2<T>) * (N + 2 * C * RL * H) + 16;  // + the table's mbarrier
+  const dim3 grow(N / RL, B);
+  const long P = (long)N * N;
+  const size_t plane = sizeof(T) * (size_t)B * C * P;
+  const int gacc = (int)std::min<long>(((long)B * P + 255) / 256, 4096);
+  const double h = (t1 - t0) / nsteps, hh = h / 2.0;
+  const double hb = -h, hhb = hb / 2.0;  // the adjoint integration runs t1 -> t0
+  const double cw[4] = {1.0, 2.0, 2.0, 1.0};
+  StageArgs af = af0, ad = ad0;
+  cudaError_t e;
+  // ---- forward integration, storing y_i at the start of each step
+  af.h = h;
+  af.stage = 0;
+  af.last = 0;
+  af.t_cur = af.t_next = t0;
+  e = launch_k<k_row<T, N, C, false, true, RL, RNT, false, RMB>>(LF_KIND_ROW, grow, RNT, smem_row, st, af);
+  if (e != cudaSuccess) return e;
+  for (int i = 0; i < nsteps; ++i) {
+    e = cudaMemcpyAsync(ckpt + (size_t)i * plane, af.y0, plane, cudaMemcpyDeviceToDevice, st);
+    if (e != cudaSuccess) return e;
+    const double t = t0 + i * h;
+    const double tc[4] = {t, t + hh, t + hh, t + h};
+    const double tn[4] = {t + hh, t + hh, t + h, t0 + (i + 1) * h};
+    for (int s = 0; s < 4; ++s) {
+      af.stage = s + 1;
+      af.t_cur = tc[s];
+      af.t_next = tn[s];
+      af.last = (i == nsteps - 1 && s == 3);
+      e = launch_col<T, N>(B * C, st, af);
+      if (e != cudaSuccess) return e;
+      e = launch_k<k_row<T, N, C, false, false, RL, RNT, false, RMB>>(LF_KIND_ROW, grow, RNT, smem_row, st, af);
+      if (e != cudaSuccess) return e;
+    }
+  }
+  // ---- adjoint initialisation from the cotangent (saves the first stage input)
+  ad.h = hb;
+  ad.stage = 0;
+  ad.last = 0;
+  ad.t_cur = ad.t_next = t1;
+  e = launch_k<k_row<T, N, C, true, true, RL, RNT, true, RMB>>(LF_KIND_ROW, grow, RNT, smem_row, st, ad);
+  if (e != cudaSuccess) return e;
+  // ---- reverse steps: recompute forward step i, then one adjoint RK4 step over it
+  StageArgs ar = af0;  // the recomputation reads the checkpoint in the compute precision
+  ar.in_f64 = ar.out_f64 = std::is_same<T, double>::value;
+  ar.f_out = sink;  // the recomputed steps' last-stage updates are discarded
+  ar.h = h;
+  for (int ib = 0; ib < nsteps; ++ib) {
+    const int i = nsteps - 1 - ib;
+    const double t = t0 + i * h;
+    const double tc[4] = {t, t + hh, t + hh, t + h};
+    const double tn[4] = {t + hh, t + hh, t + h, t0 + (i + 1) * h};
+    ar.f_in = ckpt + (size_t)i * plane;
+    ar.stage = 0;
+    ar.last = 0;
+    ar.t_cur = ar.t_next = t;
+    e = launch_k<k_row<T, N, C, false, true, RL, RNT, false, RMB>>(LF_KIND_ROW, grow, RNT, smem_row, st, ar);
+    if (e != cudaSuccess) return e;
+    for (int s = 0; s < 4; ++s) {
+      ar.stage = s + 1;
+      ar.t_cur = tc[s];
+      ar.t_next = tn[s];
+      ar.last = (s == 3);  // stage 4's update goes to the sink; no next-stage spectrum
+      ar.grad = grads + (size_t)s * 2 * plane;
+      e = launch_col<T, N>(B * C, st, ar);
+      if (e != cudaSuccess) return e;
+      e = launch_k<k_row<T, N, C, false, false, RL, RNT, true, RMB>>(LF_KIND_ROW, grow, RNT, smem_row, st, ar);
+      if (e != cudaSuccess) return e;
+    }
+    const double tb = t0 + (i + 1) * h;  // = t1 + ib * hb
+    const double tcb[4] = {tb, tb + hhb, tb + hhb, tb + hb};
+    const double tnb[4] = {tb + hhb, tb + hhb, tb + hb, t0 + i * h};
+    for (int j = 0; j < 4; ++j) {
+      // adjoint stage j + 1 (input in dsave) pairs with forward stage 4 - j at the same time
+      e = launch<k_dphi_accum<T, C>>(dim3(gacc), 256, 0, st, (const T*)(grads + (size_t)(3 - j) * 2 * plane),
+                                     (const T*)ad.dsave, (const T*)af.phi, dacc, B, P, tcb[j], hb / 6.0 * cw[j],
+                                     (int)(ib == 0 && j == 0));
+      if (e != cudaSuccess) return e;
+      ad.stage = j + 1;
+      ad.t_cur = tcb[j];
+      ad.t_next = tnb[j];
+      ad.last = (ib == nsteps - 1 && j == 3);
+      e = launch_col<T, N>(B * C, st, ad);
+      if (e != cudaSuccess) return e;
+      e = launch_k<k_row<T, N, C, true, false, RL, RNT, true, RMB>>(LF_KIND_ROW, grow, RNT, smem_row, st, ad);
+      if (e != cudaSuccess) return e;
+    }
+  }
+  return cudaSuccess;
+}
+
+template <typename T, int N>
+cudaError_t run_vjp_ckpt_c(int C, const StageArgs& af, const StageArgs& ad, char* ckpt, char* grads, void* sink,
+                           double* dacc, int B, int nsteps, double t0, double t1, cudaStream_t st) {
+  if (C == 1) return run_vjp_ckpt_n<T, N, 1>(af, ad, ckpt, grads, sink, dacc, B, nsteps, t0, t1, st);
+  if (C == 2) return run_vjp_ckpt_n<T, N, 2>(af, ad, ckpt, grads, sink, dacc, B, nsteps, t0, t1, st);
+  return run_vjp_ckpt_n<T, N, 3>(af, ad, ckpt, grads, sink, dacc, B, nsteps, t0, t1, st);
+}
+
+template <typename T>
+cudaError_t run_vjp_ckpt(int N, int C, const StageArgs& af, const StageArgs& ad, char* ckpt, char* grads, void* sink,
+                         double* dacc, int B, int nsteps, double t0, double t1, cudaStream_t st) {
+  switch (N) {
+    case 64: return run_vjp_ckpt_c<T, 64>(C, af, ad, ckpt, grads, sink, dacc, B, nsteps, t0, t1, st);
+    case 128: return run_vjp_ckpt_c<T, 128>(C, af, ad, ckpt, grads, sink, dacc, B, nsteps, t0, t1, st);
+    case 256: return run_vjp_ckpt_c<T, 256>(C, af, ad, ckpt, grads, sink, dacc, B, nsteps, t0, t1, st);
+    case 512: return run_vjp_ckpt_c<T, 512>(C, af, ad, ckpt, grads, sink, dacc, B, nsteps, t0, t1, st);
+    default: return run_vjp_ckpt_c<T, 1024>(C, af, ad, ckpt, grads, sink, dacc, B, nsteps, t0, t1, st);
+  }
+}
+
+// delta-phi from the five accumulator planes per map: sum_j m_j rfft2(acc_j)
+// (the multipliers of get_primal_derivatives_to_fourier, util.py:133-137), in
+// the Fourier layout or, for a map phi, summed through irfft2
+// (lense_flow.py:233-248).  ``spec`` holds 5 B spectra, ``dphi_f`` B more.
+cudaError_t finish_dphi(int N, int B, double* dacc, double2* spec, double2* dphi_f, void* dphi, int dphi_basis,
+                        const double2* tw64, double kbase, cudaStream_t st) {
+  cudaError_t e = run_rfft2(N, dacc, 1, B * 5, spec, tw64, st);
+  if (e != cudaSuccess) return e;
+  const long half = (long)B * N * (N / 2 + 1);
+  double2* target = dphi_basis == LF_PHI_FOURIER ? reinterpret_cast<double2*>(dphi) : dphi_f;
+  e = launch<k_dphi_combine>(dim3((unsigned)std::min<long>((half + 255) / 256, 4096)), 256, 0, st,
+                             (const double2*)spec, target, B, N, kbase);
+  if (e != cudaSuccess) return e;
+  if (dphi_basis == LF_PHI_MAP) e = run_irfft2(N, dphi_f, B, dphi, 1, spec, tw64, st);
+  return e;
+}
+
 bool aligned16(const void* p) { return (reinterpret_cast<uintptr_t>(p) & 15u) == 0; }
 
 }  // namespace
@@ -510,7 +727,9 @@ const char* lf_status_string(int s) {
     case LF_ERR_BAD_ARG: return "bad argument (null or misaligned pointer, bad direction or step count)";
     case LF_ERR_SINGULAR_MAGNIFICATION: return "det(I + t grad grad phi) <= 0 for some pixel and t in [0,1]";
     case LF_ERR_OOM: return "out of device memory";
-    case LF_ERR_TIMEOUT: return "timeout";
+    case LF_ERR_TIMEOUT:
+      return "timeout: a kernel block gave up waiting for its bulk copies; results since the last "
+             "lf_wait_timeouts reset are invalid";
     case LF_ERR_CUDA: return "CUDA error";
     case LF_ERR_WORKSPACE: return "workspace too small";
     default: return "unknown status";
@@ -530,6 +749,10 @@ int lf_plan_create(lf_plan_t* out, int nside, int ncomp, double pix_width, int p
   p->prec = precision;
   p->pix_width = pix_width;
   cudaGetDevice(&p->device);
+  if (cudaError_t fe = ensure_timeout_flag(); fe != cudaSuccess) {
+    delete p;
+    return cuda_status(fe);
+  }
   // exp(-2 pi i k / N) in float64 on the host, rounded once to the compute precision
   std::vector<double2> t64(nside);
   std::vector<float2> t32(nside);
@@ -627,6 +850,7 @@ float lf_decode_min_det(int i) {
 int lf_phi_precompute(lf_plan_t p, const void* phi, int basis, int batch, void* planes, int* min_det, void* ws,
                       size_t ws_bytes, void* stream) {
   if (!p) return LF_ERR_BAD_ARG;
+  if (timeout_recorded()) return LF_ERR_TIMEOUT;
   if (batch < 0) return LF_ERR_BAD_SHAPE;
   if (batch == 0) return LF_OK;
   if (basis != LF_PHI_MAP && basis != LF_PHI_FOURIER) return LF_ERR_BAD_ARG;
@@ -646,6 +870,7 @@ int lf_phi_precompute(lf_plan_t p, const void* phi, int basis, int batch, void* 
 int lf_lense_flow(lf_plan_t p, const void* f_in, int in_dtype, void* f_out, int out_dtype, const void* planes,
                   int batch, int nsteps, int direction, int adjoint, void* ws, size_t ws_bytes, void* stream) {
   if (!p) return LF_ERR_BAD_ARG;
+  if (timeout_recorded()) return LF_ERR_TIMEOUT;
   if (batch < 0) return LF_ERR_BAD_SHAPE;
   if ((in_dtype != LF_F32 && in_dtype != LF_F64) || (out_dtype != LF_F32 && out_dtype != LF_F64))
     return LF_ERR_BAD_DTYPE;
@@ -700,12 +925,35 @@ int lf_lense_flow(lf_plan_t p, const void* f_in, int in_dtype, void* f_out, int 
 
 int lf_wait_timeouts(int* count, int reset) {
   if (!count) return LF_ERR_BAD_ARG;
-  cudaError_t e = cudaMemcpyFromSymbol(count, g_lf_wait_timeouts, sizeof(int));
+  cudaError_t e = cudaDeviceSynchronize();
+  if (e == cudaSuccess) e = cudaMemcpyFromSymbol(count, g_lf_wait_timeouts, sizeof(int));
   if (e != cudaSuccess) return cuda_status(e);
+  if (timeout_recorded()) *count = 1;
   if (reset) {
     const int zero = 0;
     e = cudaMemcpyToSymbol(g_lf_wait_timeouts, &zero, sizeof(int));
+    std::lock_guard<std::mutex> lock(g_flag_mu);
+    if (int* h = g_host_flag.load()) *reinterpret_cast<volatile int*>(h) = 0;
   }
+  return cuda_status(e);
+}
+
+int lf_timeout_status(void) { return timeout_recorded() ? LF_ERR_TIMEOUT : LF_OK; }
+
+int lf_stream_check(void* stream) {
+  cudaError_t e = cudaStreamSynchronize(static_cast<cudaStream_t>(stream));
+  if (e != cudaSuccess) return cuda_status(e);
+  if (timeout_recorded()) return LF_ERR_TIMEOUT;
+  int dev_flag = 0;
+  e = cudaMemcpyFromSymbol(&dev_flag, g_lf_wait_timeouts, sizeof(int));
+  if (e != cudaSuccess) return cuda_status(e);
+  return dev_flag ? LF_ERR_TIMEOUT : LF_OK;
+}
+
+int lf_set_wait_polls(int polls) {
+  const int v = polls < 0 ? kWaitTries : std::min(polls, kWaitTries);
+  cudaError_t e = cudaDeviceSynchronize();
+  if (e == cudaSuccess) e = cudaMemcpyToSymbol(g_lf_wait_polls, &v, sizeof(int));
   return cuda_status(e);
 }
 
@@ -716,6 +964,7 @@ size_t lf_fft_workspace_bytes(lf_plan_t p, int batch) {
 
 int lf_rfft2(lf_plan_t p, const void* maps, int in_dtype, int batch, void* spec, void* stream) {
   if (!p) return LF_ERR_BAD_ARG;
+  if (timeout_recorded()) return LF_ERR_TIMEOUT;
   if (batch < 0) return LF_ERR_BAD_SHAPE;
   if (in_dtype != LF_F32 && in_dtype != LF_F64) return LF_ERR_BAD_DTYPE;
   if (batch == 0) return LF_OK;
@@ -728,6 +977,7 @@ int lf_rfft2(lf_plan_t p, const void* maps, int in_dtype, int batch, void* spec,
 int lf_irfft2(lf_plan_t p, const void* spec, int batch, void* maps, int out_dtype, void* ws, size_t ws_bytes,
               void* stream) {
   if (!p) return LF_ERR_BAD_ARG;
+  if (timeout_recorded()) return LF_ERR_TIMEOUT;
   if (batch < 0) return LF_ERR_BAD_SHAPE;
   if (out_dtype != LF_F32 && out_dtype != LF_F64) return LF_ERR_BAD_DTYPE;
   if (batch == 0) return LF_OK;
@@ -747,6 +997,7 @@ int lf_lense_flow_vjp(lf_plan_t p, const void* f_lensed, const void* cotangent, 
                       int batch, int nsteps, int direction, void* delta_f, void* f_back, void* dphi, int dphi_basis,
                       void* ws, size_t ws_bytes, void* stream) {
   if (!p) return LF_ERR_BAD_ARG;
+  if (timeout_recorded()) return LF_ERR_TIMEOUT;
   if (batch < 0) return LF_ERR_BAD_SHAPE;
   if (io_dtype != LF_F32 && io_dtype != LF_F64) return LF_ERR_BAD_DTYPE;
   if (nsteps < 1 || (direction != LF_FORWARD_LENSE && direction != LF_INVERSE_LENSE)) return LF_ERR_BAD_ARG;
@@ -803,17 +1054,77 @@ int lf_lense_flow_vjp(lf_plan_t p, const void* f_lensed, const void* cotangent, 
   cudaError_t e = p->prec == LF_F64 ? run_vjp<double>(p->N, p->C, af, ad, dacc, batch, nsteps, t0, t1, st)
                                     : run_vjp<float>(p->N, p->C, af, ad, dacc, batch, nsteps, t0, t1, st);
   if (e != cudaSuccess) return cuda_status(e);
-  // delta-phi = sum_j m_j rfft2(acc_j): rfft2 of the 5B accumulator planes, then combine
-  e = run_rfft2(p->N, dacc, 1, batch * 5, spec, p->tw64, st);
+  return cuda_status(finish_dphi(p->N, batch, dacc, spec, dphi_f, dphi, dphi_basis, p->tw64, af.kbase, st));
+}
+
+size_t lf_vjp_ckpt_workspace_bytes(lf_plan_t p, int batch, int nsteps) {
+  if (!p || batch < 0 || nsteps < 1) return 0;
+  return CkptLayout(p->N, p->C, batch, nsteps, p->prec == LF_F64 ? 8 : 4).total;
+}
+
+int lf_lense_flow_vjp_ckpt(lf_plan_t p, const void* f_in, const void* cotangent, int io_dtype, const void* planes,
+                           int batch, int nsteps, int direction, void* f_out, void* delta_f, void* dphi, int dphi_basis,
+                           void* ws, size_t ws_bytes, void* stream) {
+  if (!p) return LF_ERR_BAD_ARG;
+  if (timeout_recorded()) return LF_ERR_TIMEOUT;
+  if (batch < 0) return LF_ERR_BAD_SHAPE;
+  if (io_dtype != LF_F32 && io_dtype != LF_F64) return LF_ERR_BAD_DTYPE;
+  if (nsteps < 1 || (direction != LF_FORWARD_LENSE && direction != LF_INVERSE_LENSE)) return LF_ERR_BAD_ARG;
+  if (dphi_basis != LF_PHI_MAP && dphi_basis != LF_PHI_FOURIER) return LF_ERR_BAD_ARG;
+  if (batch == 0) return LF_OK;
+  if (!f_in || !cotangent || !planes || !delta_f || !dphi || !ws) return LF_ERR_BAD_ARG;
+  if (!aligned16(f_in) || !aligned16(cotangent) || !aligned16(planes) || !aligned16(delta_f) || !aligned16(dphi) ||
+      !aligned16(ws) || (f_out && !aligned16(f_out)))
+    return LF_ERR_BAD_ARG;
+  const size_t el = p->prec == LF_F64 ? 8 : 4;
+  const CkptLayout L(p->N, p->C, batch, nsteps, el);
+  if (ws_bytes < L.total) return LF_ERR_WORKSPACE;
+  // the lens being differentiated runs 0 -> 1 for direction +1 (lense_flow.py:304-322)
+  const double t0 = direction == LF_FORWARD_LENSE ? 0.0 : 1.0, t1 = 1.0 - t0;
+  const size_t plane = el * (size_t)batch * p->C * p->N * p->N;
+  char* w = reinterpret_cast<char*>(ws);
+  char* ckpt = w;
+  char* fs = ckpt + L.ckpt;
+  char* grads = fs + L.f_sys;
+  char* ds = grads + L.grads;
+  char* dsave = ds + L.d_sys;
+  char* sink = dsave + L.dsave;
+  double* dacc = reinterpret_cast<double*>(sink + L.sink);
+  double2* spec = reinterpret_cast<double2*>(reinterpret_cast<char*>(dacc) + L.dacc);
+  double2* dphi_f = reinterpret_cast<double2*>(reinterpret_cast<char*>(spec) + L.spec);
+  StageArgs af, ad;
+  std::memset(&af, 0, sizeof(af));
+  af.f_in = f_in;
+  af.f_out = f_out ? f_out : (void*)sink;
+  af.in_f64 = af.out_f64 = io_dtype == LF_F64;
+  af.phi = planes;
+  af.y0 = fs;
+  af.acc = fs + plane;
+  af.s = fs + 2 * plane;
+  af.gx = fs + 3 * plane;
+  af.twN = p->tw;
+  af.twP = p->twp;
+  af.twC = p->twc();
+  af.kbase = 2.0 * M_PI / ((double)p->N * p->pix_width);
+  af.nplanes = batch * p->C;
+  ad = af;
+  ad.f_in = cotangent;
+  ad.f_out = delta_f;
+  ad.y0 = ds;
+  ad.acc = ds + plane;
+  ad.s = ds + 2 * plane;
+  ad.v = ds + 3 * plane;
+  ad.gx = ds + 4 * plane;
+  ad.dsave = dsave;
+  cudaStream_t st = (cudaStream_t)stream;
+  g_prof = &p->prof;
+  cudaError_t e;
+  if (p->prec == LF_F64)
+    e = run_vjp_ckpt<double>(p->N, p->C, af, ad, ckpt, grads, sink, dacc, batch, nsteps, t0, t1, st);
+  else
+    e = run_vjp_ckpt<float>(p->N, p->C, af, ad, ckpt, grads, sink, dacc, batch, nsteps, t0, t1, st);
   if (e != cudaSuccess) return cuda_status(e);
-  const long half = (long)batch * p->N * (p->N / 2 + 1);
-  double2* target = dphi_basis == LF_PHI_FOURIER ? reinterpret_cast<double2*>(dphi) : dphi_f;
-  e = launch<k_dphi_combine>(dim3((unsigned)std::min<long>((half + 255) / 256, 4096)), 256, 0, st,
-                             (const double2*)spec, target, batch, p->N, af.kbase);
-  if (e != cudaSuccess) return cuda_status(e);
-  if (dphi_basis == LF_PHI_MAP)  // the map-basis reference sums irfft2 of each term (lense_flow.py:240-248)
-    e = run_irfft2(p->N, dphi_f, batch, dphi, 1, spec, p->tw64, st);
-  return cuda_status(e);
+  return cuda_status(finish_dphi(p->N, batch, dacc, spec, dphi_f, dphi, dphi_basis, p->tw64, af.kbase, st));
 }
 
 int lf_profile_enable(lf_plan_t p, int enable) {
@@ -948,18 +1259,19 @@ extern "C" int lf_lense_flow_noalloc(int nside, int ncomp, double pix_width, con
     return LF_ERR_BAD_DTYPE;
   if (!(pix_width > 0.0) || !std::isfinite(pix_width)) return LF_ERR_BAD_ARG;
   if (nsteps < 0 || (direction != LF_FORWARD_LENSE && direction != LF_INVERSE_LENSE)) return LF_ERR_BAD_ARG;
+  if (timeout_recorded()) return LF_ERR_TIMEOUT;
   const bool adj = adjoint != 0;
   const size_t npix = (size_t)nside * nside * (size_t)batch * ncomp;
   const size_t plane_bytes = 4 * npix;  // float32 compute
-  if (plane_bytes * (adj ? 5 : 4) > (size_t)LF_NOALLOC_SCRATCH_BYTES) return LF_ERR_WORKSPACE;
   if (batch == 0) return LF_OK;
   if (!f_in || !f_out || !planes || !aligned16(f_in) || !aligned16(f_out) || !aligned16(planes)) return LF_ERR_BAD_ARG;
   cudaStream_t st = (cudaStream_t)stream;
-  if (nsteps == 0) {
+  if (nsteps == 0) {  // as lf_lense_flow: the input, needing no scratch
     if (in_dtype != out_dtype) return LF_ERR_BAD_DTYPE;
     if (f_in == f_out) return LF_OK;
     return cuda_status(cudaMemcpyAsync(f_out, f_in, npix * (in_dtype == LF_F64 ? 8 : 4), cudaMemcpyDeviceToDevice, st));
   }
+  if (plane_bytes * (adj ? 5 : 4) > (size_t)LF_NOALLOC_SCRATCH_BYTES) return LF_ERR_WORKSPACE;
   NoAllocDevice* d = nullptr;
   const int s = noalloc_setup(&d);
   if (s != LF_OK) return s;

@@ -131,9 +131,19 @@ __host__ __device__ constexpr int col_tw_entries(int n, bool two = false) {
 }
 
 // ============================================ bulk copies and bounded waits
+constexpr int kWaitTries = 1 << 20;  // polls of a bounded wait: about one second
+
 // Set (never cleared by the kernels) when a block gave up waiting for its
 // bulk copies; the host reads it with lf_wait_timeouts().
 __device__ int g_lf_wait_timeouts;
+// Polls of a block's first wait on its bulk copies.  lf_set_wait_polls lowers
+// it (a test hook) so that the first wait runs out while the copies are still
+// legitimately in flight; the drain wait that follows always polls kWaitTries.
+__device__ int g_lf_wait_polls = kWaitTries;
+// Mapped pinned host word (set up per device by lf_plan_create, else null):
+// a timed-out block also sets it, so that every later entry point can report
+// LF_ERR_TIMEOUT without synchronising the device.
+__device__ int* g_lf_timeout_host;
 
 __device__ __forceinline__ uint32_t smem_addr(const void* p) {
   return static_cast<uint32_t>(__cvta_generic_to_shared(p));
@@ -176,7 +186,31 @@ __device__ __forceinline__ bool mbar_wait(uint64_t* mbar, uint32_t parity, int t
   return false;
 }
 
-constexpr int kWaitTries = 1 << 20;  // about one second
+// Record that a block stopped waiting: the device flag and, when set up, the
+// mapped host word (a plain store made visible system-wide; host-memory
+// atomics are not available over every interconnect).  Only the thread that
+// flips the device flag writes the host word, so a launch whose every block
+// times out sends one write over the interconnect, not one per thread.
+__device__ __forceinline__ void record_timeout() {
+  if (atomicExch(&g_lf_wait_timeouts, 1) != 0) return;
+  int* h = g_lf_timeout_host;
+  if (h) {
+    *reinterpret_cast<volatile int*>(h) = 1;
+    __threadfence_system();
+  }
+}
+
+// Wait for phase ``parity``.  If the first bounded wait (g_lf_wait_polls
+// polls) runs out, record the timeout -- this launch's results are then
+// invalid -- and wait once more, bounded by kWaitTries polls, for the copies
+// still in flight, so that they land before the block moves on or exits.
+// Returns whether the first wait succeeded.
+__device__ __forceinline__ bool wait_or_record(uint64_t* mbar, uint32_t parity) {
+  if (mbar_wait(mbar, parity, g_lf_wait_polls)) return true;
+  record_timeout();
+  mbar_wait(mbar, parity, kWaitTries);
+  return false;
+}
 
 // ======================================================== column pass
 // Gx = IFFT_col( (i KX / N^2) * FFT_col(S) ) on tiles of LINES columns.
@@ -204,14 +238,8 @@ __global__ void __launch_bounds__(NT, MINB) k_col(StageArgs a) {
   }
   pdl_wait();
   // after the first pass's barrier (which also orders the barrier's init before the waits)
-  auto wait_table = [=]() {
-    if (!mbar_wait(mbar, 0, kWaitTries)) {
-      // the table never arrived: record it (this launch's results are then
-      // invalid), let the copy drain, and go on to the remaining barriers
-      atomicExch(&g_lf_wait_timeouts, 1);
-      mbar_wait(mbar, 0, kWaitTries);
-    }
-  };
+  // (a timed-out table wait is recorded; the block goes on to its remaining barriers)
+  auto wait_table = [=]() { wait_or_record(mbar, 0); };
   const c2<T>* in = reinterpret_cast<const c2<T>*>(a.s) + plane * (long)N * H + c0;
   c2<T>* out = reinterpret_cast<c2<T>*>(a.gx) + plane * (long)N * H + c0;
   // i KX / N^2 between the transforms; zero on KX's Nyquist row of the packed
@@ -270,14 +298,8 @@ __global__ void __launch_bounds__(NT, MINB) k_row(StageArgs a) {
   }
   pdl_wait();
   // after the barrier that follows the row loads (it also orders the init before the waits)
-  auto wait_table = [=]() {
-    if (!mbar_wait(mbar, 0, kWaitTries)) {
-      // the table never arrived: record it (this launch's results are then
-      // invalid), let the copy drain, and go on to the remaining barriers
-      atomicExch(&g_lf_wait_timeouts, 1);
-      mbar_wait(mbar, 0, kWaitTries);
-    }
-  };
+  // (a timed-out table wait is recorded; the block goes on to its remaining barriers)
+  auto wait_table = [=]() { wait_or_record(mbar, 0); };
   const T* phi = reinterpret_cast<const T*>(a.phi) + map * 5 * P + (long)r0 * N;
   const T tnext = T(a.t_next);
   const T tcur = T(a.t_cur);
@@ -532,13 +554,9 @@ __global__ void __launch_bounds__(NT, MINB) k_row_pair(StageArgs a) {
   constexpr int O8 = ptw_offset(N, R, R), O64 = ptw_offset(N, R, R * R);
   const T ky_scale = T(a.kbase / double(N));
   __syncthreads();  // barriers initialised before anyone waits on them
-  if (!mbar_wait(mbar + 1, 0, kWaitTries)) {
-    // the pass table and spectra never arrived: record it (this launch's
-    // results are then invalid), let the copies drain, and go on so that
-    // every thread meets every barrier below
-    atomicExch(&g_lf_wait_timeouts, 1);
-    mbar_wait(mbar + 1, 0, kWaitTries);
-  }
+  // the pass table and spectra: a timed-out wait is recorded and the block goes
+  // on, so that every thread meets every barrier below
+  wait_or_record(mbar + 1, 0);
 
   // ------------------------- load: Z_c = DX_c + i DY_c with DY = i KY S / N
   // (slot 0 of a packed spectrum holds the real DC and Nyquist bins; the d_y
@@ -597,12 +615,7 @@ __global__ void __launch_bounds__(NT, MINB) k_row_pair(StageArgs a) {
   dft<R, T, true>(v[0]);
   dft<R, T, true>(v[1]);
   // v[c][r] = dx + i dy of component c at pixel n = j + NB r of row r0 + row
-  if (!mbar_wait(mbar, 0, kWaitTries)) {
-    // the staged operands never arrived: record it, let the copies drain, leave
-    atomicExch(&g_lf_wait_timeouts, 1);
-    mbar_wait(mbar, 0, kWaitTries);
-    return;
-  }
+  if (!wait_or_record(mbar, 0)) return;  // the staged operands: recorded, drained, leave
   const long prow = prow0 + (long)row * N;
   const T* sy0 = stg + row * N;
   const T* sacc = stg + 2 * RB + row * N;
@@ -738,13 +751,9 @@ __global__ void __launch_bounds__(NT, MINB) k_row_pair_adj(StageArgs a) {
   constexpr int O8 = ptw_offset(N, R, R), O64 = ptw_offset(N, R, R * R);
   const T ky_scale = T(a.kbase / double(N));
   __syncthreads();  // barriers initialised before anyone waits on them
-  if (!mbar_wait(mbar + 1, 0, kWaitTries)) {
-    // the pass table and spectra never arrived: record it (this launch's
-    // results are then invalid), let the copies drain, and go on so that
-    // every thread meets every barrier below
-    atomicExch(&g_lf_wait_timeouts, 1);
-    mbar_wait(mbar + 1, 0, kWaitTries);
-  }
+  // the pass table and spectra: a timed-out wait is recorded and the block goes
+  // on, so that every thread meets every barrier below
+  wait_or_record(mbar + 1, 0);
 
   // -------------------- load: Z = K_0 + i K_1, K_c = Gx_c + i KY V_c / N (Hermitian)
   // The packed rows sit in tiles 0 and 1; all are read before Z overwrites tile 0.
@@ -791,11 +800,7 @@ __global__ void __launch_bounds__(NT, MINB) k_row_pair_adj(StageArgs a) {
   for (int r = 1; r < R; ++r) z[r] = twmul<T, true>(z[r], tw[O64 + (r - 1) * NB + j]);
   dft<R, T, true>(z);
   // z[r] = (k_0, k_1) at pixel n = j + NB r of row r0 + row
-  if (!mbar_wait(mbar, 0, kWaitTries)) {
-    atomicExch(&g_lf_wait_timeouts, 1);
-    mbar_wait(mbar, 0, kWaitTries);
-    return;
-  }
+  if (!wait_or_record(mbar, 0)) return;  // the staged operands: recorded, drained, leave
   const long prow = prow0 + (long)row * N;
   const T* sy0 = stg + row * N;
   const T* sacc = stg + 2 * RB + row * N;
@@ -914,14 +919,8 @@ __device__ __forceinline__ void table_copy(double2* tw, const double2* src, uint
   }
 }
 
-__device__ __forceinline__ void table_wait(uint64_t* mbar) {
-  if (!mbar_wait(mbar, 0, kWaitTries)) {
-    // the table never arrived: record it (this launch's results are then
-    // invalid), let the copy drain, and go on to the remaining barriers
-    atomicExch(&g_lf_wait_timeouts, 1);
-    mbar_wait(mbar, 0, kWaitTries);
-  }
-}
+// (a timed-out wait is recorded; the block goes on to its remaining barriers)
+__device__ __forceinline__ void table_wait(uint64_t* mbar) { wait_or_record(mbar, 0); }
 // rfft along rows of a real map (N x N double) into the unpacked
 // (N x (N/2+1)) complex layout of rfft2.   grid: x = row tile, y = map.
 template <int N, int LINES, int NT, typename TI = double>

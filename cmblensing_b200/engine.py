@@ -101,6 +101,7 @@ class Plan:
                       "lf_phi_precompute")
         if md is not None:
             vals = [self._lib.lf_decode_min_det(int(v)) for v in md.cpu().tolist()[:B]]
+            check_timeouts("lf_phi_precompute")
             self.last_min_det = vals
             if not all(v > 0.0 for v in vals):
                 raise nat.SingularMagnificationError(nat.LF_ERR_SINGULAR_MAGNIFICATION,
@@ -204,6 +205,42 @@ class Plan:
                                                   _ptr(ws), ws.numel(), _stream_ptr(self.device)),
                       "lf_lense_flow_vjp")
         return (df, dphi, fb) if return_f else (df, dphi)
+
+    def lense_flow_vjp_ckpt(self, f, cotangent, planes, n=10, direction=FORWARD_LENSE, phi_basis="fourier",
+                            return_lensed=False):
+        """Checkpointed exact reverse pass (lf_lense_flow_vjp_ckpt) from the UNLENSED fields f [B,C,N,N].
+
+        The forward integration keeps one field per RK4 step; each step is
+        recomputed from it on the way back, so delta_phi is the exact gradient
+        of the discrete lens (the reference scheme of ``lense_flow_vjp``
+        carries the RK4 discretisation error).  Returns (delta_f, delta_phi[,
+        lensed]) in the conventions of ``lense_flow_vjp``.
+        """
+        N, C = self.nside, self.ncomp
+        if f.shape != cotangent.shape or f.dim() != 4 or f.shape[1:] != (C, N, N):
+            raise nat.LenseFlowError(nat.LF_ERR_BAD_SHAPE, "field/cotangent shapes")
+        dt = torch.float64 if torch.float64 in (f.dtype, cotangent.dtype) else torch.float32
+        fi = f.to(dt).contiguous()
+        ct = cotangent.to(dt).contiguous()
+        B = fi.shape[0]
+        if planes.shape != (B, 5, N, N) or planes.dtype != self.dtype:
+            raise nat.LenseFlowError(nat.LF_ERR_BAD_SHAPE, "phi planes do not match")
+        df = torch.empty_like(fi)
+        lensed = torch.empty_like(fi) if return_lensed else None
+        fourier = phi_basis == "fourier"
+        dphi = (torch.empty((B, N, N // 2 + 1), dtype=torch.complex128, device=self.device) if fourier
+                else torch.empty((B, N, N), dtype=torch.float64, device=self.device))
+        ws = torch.empty(max(int(self._lib.lf_vjp_ckpt_workspace_bytes(self.handle, B, int(n))), 16),
+                         dtype=torch.uint8, device=self.device)
+        code = nat.LF_F64 if dt == torch.float64 else nat.LF_F32
+        with torch.cuda.device(self.device):
+            nat.check(self._lib.lf_lense_flow_vjp_ckpt(self.handle, _ptr(fi), _ptr(ct), code, _ptr(planes), B, int(n),
+                                                       int(direction), _ptr(lensed) if lensed is not None else None,
+                                                       _ptr(df), _ptr(dphi),
+                                                       nat.LF_PHI_FOURIER if fourier else nat.LF_PHI_MAP, _ptr(ws),
+                                                       ws.numel(), _stream_ptr(self.device)),
+                      "lf_lense_flow_vjp_ckpt")
+        return (df, dphi, lensed) if return_lensed else (df, dphi)
 
     # ---------------------------------------------------------- profiling
     def profile(self, enable=True):
@@ -328,6 +365,7 @@ class HostPipeline:
         events = self._pending.pop(ring)
         for ev in events:
             ev.synchronize()
+        check_timeouts("HostPipeline")
         lib = self.plan._lib
         vals = [lib.lf_decode_min_det(int(v)) for v in self.min_det[ring][:self.batch].cpu().tolist()]
         self.plan.last_min_det = vals
@@ -340,6 +378,10 @@ class HostPipeline:
         cur = torch.cuda.current_stream(self.plan.device)
         for st in [self.s_in, self.s_out] + self.s_cmp:
             cur.wait_stream(st)
+        if not self._pending:  # calls without the magnification check: wait for the compute here
+            for st in self.s_cmp:
+                st.synchronize()
+            check_timeouts("HostPipeline")
         err = None
         for ring in sorted(self._pending):
             try:
@@ -425,52 +467,71 @@ class LenseFlowFunction(torch.autograd.Function):
     """torch autograd for y = L(phi) f on device tensors.
 
     f: [B,C,N,N]; phi: [B,N,N] real map or [B,N,N/2+1] complex Fourier.
-    The backward pass is the reference's scheme (lense_flow.py:23-126): the
-    f-cotangent is the exact adjoint lens of the incoming gradient, the
-    phi-cotangent the continuous adjoint integrated with RK4 (it matches the
-    exact discrete gradient to the RK4 discretisation error).  For a complex
-    Fourier phi the gradient follows torch's convention dL/dRe + i dL/dIm,
-    i.e. the reference's delta-phi times w/N^2 (w = 1 on the DC/Nyquist
-    columns, 2 elsewhere).
+    ``scheme="reference"``: the reference's backward pass (lense_flow.py:
+    23-126): the f-cotangent is the exact adjoint lens of the incoming
+    gradient, the phi-cotangent the continuous adjoint integrated with RK4 (it
+    matches the exact discrete gradient to the RK4 discretisation error).
+    ``scheme="exact"``: the checkpointed reverse pass (lf_lense_flow_vjp_ckpt):
+    same f-cotangent, and the exact gradient of the discrete lens for phi.
+    For a complex Fourier phi the gradient follows torch's convention
+    dL/dRe + i dL/dIm, i.e. the reference's delta-phi times w/N^2 (w = 1 on
+    the DC/Nyquist columns, 2 elsewhere).
     """
 
     @staticmethod
-    def forward(ctx, f, phi, pix_width, n, direction, precision):
+    def forward(ctx, f, phi, pix_width, n, direction, precision, scheme="reference"):
+        if scheme not in ("reference", "exact"):
+            raise ValueError(f"unknown reverse-pass scheme {scheme!r}")
         plan = get_plan(f.shape[-1], f.shape[1], pix_width, precision, device=f.device)
         planes = plan.phi_planes(phi.detach(), check_det=False)
         out = plan.lense_flow(f.detach(), planes, n=n, direction=direction)
-        ctx.save_for_backward(out, planes)
-        ctx.plan, ctx.n, ctx.direction = plan, n, direction
+        ctx.save_for_backward(f.detach() if scheme == "exact" else out, planes)
+        ctx.plan, ctx.n, ctx.direction, ctx.scheme = plan, n, direction, scheme
         ctx.fourier = phi.is_complex()
         ctx.phi_dtype, ctx.f_dtype = phi.dtype, f.dtype
         return out
 
     @staticmethod
     def backward(ctx, g):
-        out, planes = ctx.saved_tensors
+        saved, planes = ctx.saved_tensors
         plan = ctx.plan
-        df, dphi = plan.lense_flow_vjp(out, g.contiguous(), planes, n=ctx.n, direction=ctx.direction,
-                                       phi_basis="fourier" if ctx.fourier else "map")
+        basis = "fourier" if ctx.fourier else "map"
+        if ctx.scheme == "exact":
+            df, dphi = plan.lense_flow_vjp_ckpt(saved, g.contiguous(), planes, n=ctx.n, direction=ctx.direction,
+                                                phi_basis=basis)
+        else:
+            df, dphi = plan.lense_flow_vjp(saved, g.contiguous(), planes, n=ctx.n, direction=ctx.direction,
+                                           phi_basis=basis)
         if ctx.fourier:
             N = plan.nside
             w = torch.full((N // 2 + 1,), 2.0, dtype=torch.float64, device=dphi.device)
             w[0] = 1.0
             w[-1] = 1.0
             dphi = dphi * (w / (N * N))
-        return df.to(ctx.f_dtype), dphi.to(ctx.phi_dtype), None, None, None, None
+        return df.to(ctx.f_dtype), dphi.to(ctx.phi_dtype), None, None, None, None, None
 
 
-def lense_flow_ad(f, phi, pix_width, n=10, direction=FORWARD_LENSE, precision="f32"):
-    """Differentiable LenseFlow (torch autograd) on device tensors."""
-    return LenseFlowFunction.apply(f, phi, pix_width, n, direction, precision)
+def lense_flow_ad(f, phi, pix_width, n=10, direction=FORWARD_LENSE, precision="f32", scheme="reference"):
+    """Differentiable LenseFlow (torch autograd) on device tensors; ``scheme`` selects the reverse pass."""
+    return LenseFlowFunction.apply(f, phi, pix_width, n, direction, precision, scheme)
 
 
 def wait_timeouts(reset=False):
-    """1 if a kernel block gave up waiting for its bulk copies since the last reset (its results are invalid)."""
-    import ctypes
+    """1 if a kernel block gave up waiting for its bulk copies since the last reset (its results are invalid).
+
+    Synchronises the device; ``reset`` clears the record, after which the entry points compute again."""
     count = ctypes.c_int(0)
     nat.check(nat.load().lf_wait_timeouts(ctypes.byref(count), int(bool(reset))), "lf_wait_timeouts")
     return count.value
+
+
+def check_timeouts(what="LenseFlow"):
+    """Raise LenseFlowError(LF_ERR_TIMEOUT) if a kernel block has recorded a timed-out wait.
+
+    No synchronisation: call it after the work in question has been waited for
+    (the synchronising paths -- HostPipeline.wait, the server's batch
+    completion, the Wiener filter's convergence checks -- do)."""
+    nat.check(nat.load().lf_timeout_status(), what)
 
 
 def get_plan(nside, ncomp, pix_width, precision="f32", device=None):

@@ -42,23 +42,26 @@ def _weight_ratio(nside, weights, like):
 
 @on_device
 def grad_phi_logpdf(unlensed_field, phi, data, noise_covariance, phi_covariance, field_covariance, mask, beam,
-                    n=10):
+                    n=10, scheme="reference", precision="f32"):
     """d logpdf / d phi for a Fourier phi: jax.grad(logpdf, argnums=1) of gradients.py:30-37, by hand.
 
     The data term's cotangent w.r.t. the lensed map is the ordinary partial
     derivative irfft2(eb2qu(B M Cn^-1 (d - M B L f)) * w / w_std), which the
     engine's reverse pass (the reference's custom VJP, lense_flow.py:23-46)
     turns into a Fourier delta-phi; the phi prior's custom VJP
-    (statistics.py:199-209) adds -Cphi^-1 phi.
+    (statistics.py:199-209) adds -Cphi^-1 phi.  ``scheme="exact"`` uses the
+    checkpointed reverse pass instead: the exact gradient of the discrete
+    lens, without the reference scheme's RK4 discretisation gap.
     """
     fmap = map(eb2qu(unlensed_field))
-    lensed_map = lense_flow(fmap, phi, n=n)
+    lensed_map = lense_flow(fmap, phi, n=n, precision=precision)
     resid = data - mask * beam * qu2eb(fourier(lensed_map))
     h = eb2qu(beam * mask * (pinv(noise_covariance) * resid))
     names = h._matrix_names()
     ratio = _weight_ratio(data.nside, resid.fourier_weights, getattr(h, names[0]))
     cot = map(h.replace(**{nm: getattr(h, nm) * ratio for nm in names}))
-    _, dphi = lense_flow_backwards(lensed_map, phi, cot, n=n, direction=FORWARD_LENSE)
+    _, dphi = lense_flow_backwards(lensed_map, phi, cot, n=n, direction=FORWARD_LENSE, precision=precision,
+                                   scheme=scheme, field=fmap)
     prior = pinv(phi_covariance) * phi
     return dphi.replace(scalar_matrix=dphi.scalar_matrix - prior.scalar_matrix, fourier_weights=phi.fourier_weights,
                         basis=Basis.FOURIER, parametrization=Parametrization.T)

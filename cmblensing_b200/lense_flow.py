@@ -40,6 +40,7 @@ def lense_flow(field, phi, n=10, direction=1, adjoint=False, precision="f32"):
                                   precision=precision)
     if host:
         arr = out[0].to(torch.float64).cpu().numpy()
+        engine.check_timeouts("lense_flow")
         upd = {nm: arr[i] for i, nm in enumerate(names)}
     else:
         upd = {nm: out[0, i] for i, nm in enumerate(names)}
@@ -52,7 +53,8 @@ def _stack(field, dev):
     return t if t.dtype in (torch.float32, torch.float64) else t.real.to(torch.float64)
 
 
-def lense_flow_backwards(transformed_field, phi, cotangent, n=10, direction=1, swap_qu=True, precision="f32"):
+def lense_flow_backwards(transformed_field, phi, cotangent, n=10, direction=1, swap_qu=True, precision="f32",
+                         scheme="reference", field=None):
     """The reference's custom-VJP backward pass (cmb_lensing/lense_flow.py:23-46).
 
     Integrates (f, delta_f, delta_phi) from the lensed field in the opposite
@@ -61,6 +63,11 @@ def lense_flow_backwards(transformed_field, phi, cotangent, n=10, direction=1, s
     With ``swap_qu`` the Q/U matrices of delta_field are returned swapped, as
     the reference's output_like_input writes them (lense_flow.py:143-144,
     151-152); pass ``swap_qu=False`` for the mathematically ordered result.
+    ``scheme="exact"`` runs the checkpointed reverse pass instead
+    (lf_lense_flow_vjp_ckpt): it needs ``field``, the unlensed MAP-basis field
+    that ``transformed_field`` came from (the reference's VJP residuals hold it
+    too, lense_flow.py:10-21), and returns the exact gradient of the discrete
+    lens for delta_phi.
     """
     from .fields import FlatS0, undo_inner_product
     names = transformed_field._matrix_names()
@@ -74,11 +81,22 @@ def lense_flow_backwards(transformed_field, phi, cotangent, n=10, direction=1, s
     pm = pm.to(torch.complex128) if fourier_phi else pm.to(torch.float64)
     plan = engine.get_plan(fl.shape[-1], fl.shape[1], phi.pix_width, precision, device=dev)
     planes = plan.phi_planes(pm.unsqueeze(0), check_det=False)
-    df, dphi = plan.lense_flow_vjp(fl, ct, planes, n=n, direction=direction,
-                                   phi_basis="fourier" if fourier_phi else "map")
+    basis = "fourier" if fourier_phi else "map"
+    if scheme == "exact":
+        if field is None:
+            raise ValueError("scheme='exact' needs the unlensed field (field=...)")
+        df, dphi = plan.lense_flow_vjp_ckpt(_stack(field, dev).to(torch.float64), ct, planes, n=n,
+                                            direction=direction, phi_basis=basis)
+    elif scheme == "reference":
+        df, dphi = plan.lense_flow_vjp(fl, ct, planes, n=n, direction=direction, phi_basis=basis)
+    else:
+        raise ValueError(f"unknown reverse-pass scheme {scheme!r}")
     comps = [df[0, i] for i in range(len(names))]
     if swap_qu and not isinstance(transformed_field, FlatS0):
         comps[-2], comps[-1] = comps[-1], comps[-2]
+    if host:
+        torch.cuda.current_stream(dev).synchronize()
+        engine.check_timeouts("lense_flow_backwards")
     conv = (lambda t: t.cpu().numpy()) if host else (lambda t: t)
     dfield = transformed_field.replace(**{nm: conv(c) for nm, c in zip(names, comps)})
     dphi_field = phi.replace(scalar_matrix=conv(dphi[0]))

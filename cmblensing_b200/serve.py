@@ -154,12 +154,15 @@ class _LensSlot:
             return []
         lib = self.plan._lib
         now = time.perf_counter()
+        timed_out = lib.lf_timeout_status() != nat.LF_OK
         out = self.h_out[:len(self.reqs)].numpy().copy()
         mds = self.h_md[:len(self.reqs)].tolist()
         done = self.reqs
         for i, r in enumerate(done):
             md = lib.lf_decode_min_det(int(mds[i]))
-            if not md > 0.0:
+            if timed_out:
+                r.error = nat.LenseFlowError(nat.LF_ERR_TIMEOUT, "lens batch")
+            elif not md > 0.0:
                 r.error = nat.SingularMagnificationError(nat.LF_ERR_SINGULAR_MAGNIFICATION, f"min det {md:.3g}")
             else:
                 r.result = out[i]

@@ -282,6 +282,7 @@ class DeviceWienerFilter:
                     active = active & ~(rn < rel_tol)
                 if not bool(active.any()):
                     break
+                engine.check_timeouts("Wiener filter")
             Ap = self.apply_A(p)
             pAp = self.dot(p, Ap)
             alpha = torch.where(active, res / torch.where(pAp != 0, pAp, torch.ones_like(pAp)), torch.zeros_like(res))
@@ -297,9 +298,11 @@ class DeviceWienerFilter:
             beta = torch.where(active, res_new / torch.where(res != 0, res, torch.ones_like(res)), torch.zeros_like(res))
             p = z + bc(beta) * p
             res = torch.where(active, res_new, res)
+        its = iters.cpu().tolist()
+        engine.check_timeouts("Wiener filter")
         if self.batch == 1:
-            return x[0], int(iters[0])
-        return x, iters.cpu().tolist()
+            return x[0], its[0]
+        return x, its
 
     def to_field(self, x, i=0):
         """Solution ``i`` (or the only one) as a reference-shaped field on the host."""

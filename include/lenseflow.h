@@ -123,17 +123,40 @@ int lf_lense_flow_vjp(lf_plan_t plan, const void* f_lensed, const void* cotangen
                       int batch, int nsteps, int direction, void* delta_f, void* f_back, void* dphi, int dphi_basis,
                       void* workspace, size_t workspace_bytes, void* stream);
 
+/* Checkpointed exact reverse pass: the transpose of the discrete forward map
+ * f -> L(phi) f that lf_lense_flow computes (direction +1 or -1, standard
+ * RHS), for the cotangent ``cotangent`` and the UNLENSED field ``f_in`` -- the
+ * residuals of the reference's custom VJP include f (lense_flow.py:10-51).
+ * The forward integration stores one checkpoint (the field at the start of
+ * every RK4 step) in the workspace; backwards, each step is recomputed from
+ * its checkpoint and one RK4 step of the adjoint RHS carries the cotangent
+ * over it, with delta-phi accumulated from the recomputed forward stage
+ * inputs.  delta_f equals the reference's (the adjoint lens is already the
+ * exact transpose); delta_phi is the exact gradient of the discrete map,
+ * where the reference's reverse ODE (lf_lense_flow_vjp) differs from it by the
+ * RK4 discretisation error.  Same conventions and layouts as
+ * lf_lense_flow_vjp; ``f_out`` (optional) receives L(phi) f_in.  Extends the
+ * reference's lense_flow_backwards (lense_flow.py:23-46); the reference has
+ * no checkpointed scheme. */
+size_t lf_vjp_ckpt_workspace_bytes(lf_plan_t plan, int batch, int nsteps);
+int lf_lense_flow_vjp_ckpt(lf_plan_t plan, const void* f_in, const void* cotangent, int io_dtype, const void* planes,
+                           int batch, int nsteps, int direction, void* f_out, void* delta_f, void* dphi, int dphi_basis,
+                           void* workspace, size_t workspace_bytes, void* stream);
+
 /* Allocation-free variant of lf_lense_flow (float32 compute), for callers
  * that cannot allocate device memory: a host framework that has already
  * reserved (nearly) all of the GPU's memory for its own pool, where one more
  * cudaMalloc can fail, and latency-critical loops where cudaMalloc/cudaFree
  * would synchronise the device.  No counterpart in the reference.
- * The caller passes the inputs (fields, derivative planes from
- * lf_phi_precompute) and the output; there is no plan: the geometry is
- * passed directly.  Scratch lives in a file-scope device array of
+ * The caller passes the inputs and the output; there is no plan: the
+ * geometry is passed directly.  ``planes`` must be the float32 derivative
+ * planes [batch][5][N][N] that lf_phi_precompute wrote for a plan created
+ * with LF_F32 and the same N and pix_width (the computation is float32; the
+ * planes of a float64 plan would be misread).  Scratch lives in a file-scope device array of
  * LF_NOALLOC_SCRATCH_BYTES that every GPU which loads the library holds until
  * exit; a call needing more (4 bytes x N^2 x batch x ncomp x (4, or 5 when
- * adjoint)) returns LF_ERR_WORKSPACE.  The first call on each device resolves
+ * adjoint)) returns LF_ERR_WORKSPACE (nsteps = 0 needs none: it copies the
+ * input, as lf_lense_flow does).  The first call on each device resolves
  * the array's device address and fills twiddle tables with a synchronous
  * copy: make that first call before any stream capture.  Every call shares
  * the one array, so calls that overlap on the GPU (other streams, other host
@@ -144,17 +167,46 @@ int lf_lense_flow_noalloc(int nside, int ncomp, double pix_width, const void* f_
                           int out_dtype, const void* planes, int batch, int nsteps, int direction, int adjoint,
                           void* stream);
 
+/* Device-wait timeouts.  Every wait of a kernel block on its own bulk copies
+ * into shared memory is bounded (about one second of polls).  A block whose
+ * wait runs out records it, waits once more (bounded) for its copies in
+ * flight and then skips or finishes its work: the results of that launch and
+ * of everything computed from them are invalid.  The record is sticky: from
+ * then on every computing entry point (lf_phi_precompute, lf_lense_flow,
+ * lf_lense_flow_vjp, lf_rfft2, lf_irfft2, lf_lense_flow_noalloc) returns
+ * LF_ERR_TIMEOUT without launching anything, until lf_wait_timeouts resets
+ * it.  Because calls are asynchronous, the call whose kernels timed out has
+ * usually returned LF_OK already; the next call, lf_timeout_status after the
+ * caller has synchronised with the work, or lf_stream_check reports it.  (If
+ * the second wait also ran out, the block may have exited with copies into
+ * its shared memory still in flight; every result until the reset is
+ * invalid in that case too.)  No counterpart in the reference (its XLA path
+ * has no device-side waits).
+ *
+ * lf_wait_timeouts: synchronises the current device, sets *count to 1 if a
+ * timeout was recorded (else 0) and, with reset != 0, clears the record.
+ * lf_timeout_status: LF_ERR_TIMEOUT if a timeout has been recorded, else
+ * LF_OK; no synchronisation (exact once the caller has synchronised with the
+ * work in question).  The record lives in one mapped pinned host word that
+ * lf_plan_create sets up; without a plan only lf_wait_timeouts and
+ * lf_stream_check see timeouts.
+ * lf_stream_check: synchronises ``stream`` and returns LF_ERR_TIMEOUT,
+ * LF_ERR_CUDA (a failed launch or fault) or LF_OK.
+ * lf_set_wait_polls: a test hook that sets the poll limit of every block's
+ * first wait on the current device (polls < 0 restores the default).  With 0
+ * the first wait runs out at once while the copies are still legitimately in
+ * flight; the drain wait keeps its full limit, so nothing waits forever and
+ * every copy lands before its block moves on.  Synchronises the device. */
+int lf_wait_timeouts(int* count, int reset);
+int lf_timeout_status(void);
+int lf_stream_check(void* stream);
+int lf_set_wait_polls(int polls);
+
 /* Launch timing for benchmarks and profiling.  While enabled, every kernel
  * launched through ``plan`` is bracketed by a CUDA event pair on its stream.
  * lf_profile_read synchronises on the last event and returns the summed
  * duration and count of the recorded launches of one kind.  No counterpart
  * in the reference (its device work is XLA-generated). */
-/* Set to 1 (and kept) if a kernel block stopped waiting for its own bulk
- * copies into shared memory after its bounded number of polls; that block
- * skipped its work, so results computed since the last reset are invalid.
- * Synchronises the current device.  No counterpart in the reference (its
- * XLA path has no device-side waits). */
-int lf_wait_timeouts(int* count, int reset);
 
 enum lf_kernel_kind { LF_KIND_ROW = 0, LF_KIND_COL = 1, LF_KIND_PHI = 2, LF_KIND_PP = 3 };
 int lf_profile_enable(lf_plan_t plan, int enable);

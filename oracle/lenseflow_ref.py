@@ -598,6 +598,64 @@ def get_lensing_operator_gradients(phi_matrix, pix_width, tqu_field, tqu_cotange
     return rk4_solve(step, y0, t0, t1, n)
 
 
+def lensing_operator_gradients_exact(phi_matrix, pix_width, tqu_field, tqu_cotangent, direction, n):
+    """The exact transpose of the discrete forward RK4 lens (the engine's checkpointed reverse pass).
+
+    No counterpart in the reference: this restates the engine's extension
+    ``lf_lense_flow_vjp_ckpt`` so that the tests can check it.  ``tqu_field``
+    is the UNLENSED (T, Q, U) map and ``direction`` the direction of the lens
+    being differentiated.  The forward RK4 (util.py:184-199 with the standard
+    RHS, lense_flow.py:365-370) keeps y_i at the start of every step; each
+    step is recomputed backwards from it, one RK4 step of the adjoint RHS
+    (lense_flow.py:355-362, with the negated step) carries the cotangent over
+    it, and forward stage s pairs with adjoint stage 5 - s at the same time:
+    delta-phi gains h_back/6 {1,2,2,1}_j get_delta_phi_tqu_roc(u_{5-j}, v_j)
+    with u the forward stage inputs and v the adjoint ones.  Pinned by central
+    finite differences of the discrete lens (tests/test_oracle_golden.py).
+    Returns (t, q, u lensed, delta_t, delta_q, delta_u, delta_phi).
+    """
+    t0, t1 = time_span(direction, False)
+    h = (t1 - t0) / n
+    hb = -h
+    phi_fourier = phi_matrix.shape[0] != phi_matrix.shape[1]
+    derivs = phi_derivatives(phi_matrix, pix_width)
+    A = lambda y, t: get_standard_lensing_term(y, *derivs, t, pix_width)
+    G = lambda y, t: get_adjoint_lensing_term(y, *derivs, t, pix_width)
+
+    def stage_inputs(y, t):
+        k1 = [A(c, t) for c in y]
+        u2 = [c + h / 2 * k for c, k in zip(y, k1)]
+        k2 = [A(c, t + h / 2) for c in u2]
+        u3 = [c + h / 2 * k for c, k in zip(y, k2)]
+        k3 = [A(c, t + h / 2) for c in u3]
+        u4 = [c + h * k for c, k in zip(y, k3)]
+        k4 = [A(c, t + h) for c in u4]
+        return [y, u2, u3, u4], [c + h / 6 * (a + 2 * b + 2 * cc + d) for c, a, b, cc, d in zip(y, k1, k2, k3, k4)]
+
+    y = [np.asarray(c, dtype=np.float64) for c in tqu_field]
+    checkpoints = []
+    for i in range(n):
+        checkpoints.append(y)
+        y = stage_inputs(y, t0 + i * h)[1]
+    lensed = y
+    dphi = np.zeros(phi_matrix.shape, dtype=np.complex128 if phi_fourier else np.float64)
+    v = [np.asarray(c, dtype=np.float64) for c in tqu_cotangent]
+    weights = (1.0, 2.0, 2.0, 1.0)
+    for i in reversed(range(n)):
+        t = t0 + i * h
+        us = stage_inputs(checkpoints[i], t)[0]
+        taus = (t + h, t + h / 2, t + h / 2, t)
+        vs, ks = [], []
+        for j in range(4):
+            vj = v if j == 0 else [a + (hb if j == 3 else hb / 2) * k for a, k in zip(v, ks[-1])]
+            vs.append(vj)
+            ks.append([G(c, taus[j]) for c in vj])
+            dphi = dphi + hb / 6 * weights[j] * get_delta_phi_tqu_roc(*us[3 - j], *vj, *derivs, taus[j], pix_width,
+                                                                      phi_fourier)
+        v = [a + hb / 6 * (p + 2 * q + 2 * r + s) for a, p, q, r, s in zip(v, *ks)]
+    return (*lensed, *v, dphi)
+
+
 def lense_flow_backwards(transformed_field, phi, cotangent, n=10, direction=1):
     """lense_flow.py:23-46: (delta_field, delta_phi) after undo_inner_product."""
     tqu = spin_vector_matrix_data(transformed_field)
@@ -643,7 +701,8 @@ def _half_plane_weight_ratio(nside, fourier_weights):
     return np.real(fourier_weights / w_std)
 
 
-def grad_phi_logpdf(field, phi, data, noise_covariance, phi_covariance, field_covariance, mask, beam, n=10):
+def grad_phi_logpdf(field, phi, data, noise_covariance, phi_covariance, field_covariance, mask, beam, n=10,
+                    scheme="reference"):
     """gradients.py:30-37: ``jax.grad(logpdf, argnums=1)`` restated by hand.
 
     The data term's cotangent w.r.t. the lensed QU/T map (a real array, so
@@ -651,7 +710,9 @@ def grad_phi_logpdf(field, phi, data, noise_covariance, phi_covariance, field_co
     ``irfft2(eb2qu(B M Cn^-1 diff) * w / w_std)``; it is fed to the
     reference's custom VJP (lense_flow.py:23-46) with phi in Fourier space.
     The phi prior's custom VJP (statistics.py:199-209) contributes
-    ``-1/2 * 2 Cphi^-1 phi``.
+    ``-1/2 * 2 Cphi^-1 phi``.  ``scheme="exact"`` replaces the reverse pass
+    with ``lensing_operator_gradients_exact`` (the engine's checkpointed
+    extension; no reference counterpart).
     """
     fmap = map_(eb2qu(field))
     lensed_map = lense_flow(fmap, phi, n=n)
@@ -663,7 +724,12 @@ def grad_phi_logpdf(field, phi, data, noise_covariance, phi_covariance, field_co
     N = data.nside
     cot = h.replace(**{nm: np.fft.irfft2(getattr(h, nm) * ratio, s=(N, N)) for nm in h._matrix_names()},
                     basis=Basis.MAP)
-    _, dphi = lense_flow_backwards(lensed_map, phi, cot, n=n, direction=FORWARD_LENSE)
+    if scheme == "exact":
+        res = lensing_operator_gradients_exact(phi.scalar_matrix, phi.pix_width, spin_vector_matrix_data(fmap),
+                                               spin_vector_matrix_data(cot), FORWARD_LENSE, n)
+        dphi = undo_inner_product(phi.replace(scalar_matrix=res[6]))
+    else:
+        _, dphi = lense_flow_backwards(lensed_map, phi, cot, n=n, direction=FORWARD_LENSE)
     prior = pinv(phi_covariance) * phi
     return dphi.scalar_matrix - prior.scalar_matrix
 

@@ -57,6 +57,11 @@ def test_null_plan_calls_return_status(lib):
     assert lib.lf_plan_destroy(None) == nat.LF_OK
 
 
+def test_timeout_status_without_a_plan(lib):
+    """No plan, no recorded timeout: the status word reads OK without touching the device."""
+    assert lib.lf_timeout_status() == nat.LF_OK
+
+
 def test_min_det_encoding_round_trip(lib):
     import struct
     for v in (0.7, 1.0, 1e-9, -0.3, -5.0, 3.4e38):

@@ -7,8 +7,12 @@ reference (tolerance 2e-5) and against central finite differences of
 logpdf (eps = 1e-3 rms) along 16 seeded directions.  For f, logpdf is
 quadratic and the gradient uses the exact discrete adjoint: 1e-4.  For phi,
 the reference's continuous delta-phi adjoint differs from the exact
-derivative by the RK4 discretisation error: 5e-3.  Directions are seeded
-Gaussian random fields with the workload's spectra.
+derivative by the RK4 discretisation error: 5e-3.  The checkpointed exact
+reverse pass (scheme="exact") has no such gap: with the FP64 engine its phi
+gradient equals Richardson-extrapolated central differences at the same eps
+to 1e-6, and its FP32 gradient matches the oracle's exact restatement to
+2e-5.  Directions are seeded Gaussian random fields with the workload's
+spectra.
 
 Wiener-filter workload: 512^2 QU, 2' pixels, 1' beam, 2 uK-arcmin noise, a
 pixel mask with 30 apodised holes, B-mode prior at 1% of C_EE (the
@@ -253,3 +257,54 @@ def test_batched_wiener_filter_equals_solo_solves(torch_cuda):
         solo = DeviceWienerFilter(problems=[pr], n=7)
         xs, _ = solo.solve(rel_tol=1e-9, refine_every=10)
         assert rel_l2(xb[i].cpu().numpy(), xs.cpu().numpy()) < 1e-7, (i, its)
+
+
+def test_grad_phi_exact_scheme_256_IQU(torch_cuda):
+    """grad_phi_logpdf with the checkpointed exact reverse pass: FP64 engine vs Richardson-extrapolated central
+    differences (eps = 1e-3 rms and 5e-4 rms, 16 directions) to 1e-6; FP32 engine vs the oracle's exact scheme at
+    128^2 to 2e-5."""
+    import cmblensing_b200 as cl
+    from cmblensing_b200 import matrix_operators as mo
+    from cmblensing_b200.gradients import grad_phi_logpdf
+    from cmblensing_b200.statistics import logpdf
+
+    class Mod:
+        FlatS0, FlatS2, FlatS02 = cl.FlatS0, cl.FlatS2, cl.FlatS02
+        DiagonalScalar, DiagonalEB, BlockTEB = mo.DiagonalScalar, mo.DiagonalEB, mo.BlockTEB
+
+    S = _problem(Mod, 256, 3.0, "IP", 3.0, 10.0, 14.0, seed=1)
+    f, phi, d = S["field"], S["phi"], S["data"]
+    args = (d, S["Cn"], S["Cphi"], S["Cf"], S["M"], S["B"])
+    gp = grad_phi_logpdf(f, phi, *args, n=7, scheme="exact", precision="f64")
+    gp_ref = grad_phi_logpdf(f, phi, *args, n=7, scheme="reference", precision="f64")
+
+    def lp(pp):
+        from cmblensing_b200 import lense_flow as lfm
+        old = lfm.engine.lense_flow_batch
+        try:
+            lfm.engine.lense_flow_batch = lambda *a, **k: old(*a, **{**k, "precision": "f64"})
+            return logpdf(f, pp, d, S["Cn"], S["Cphi"], S["Cf"], S["M"], S["B"], n=7)
+        finally:
+            lfm.engine.lense_flow_batch = old
+
+    rms_p = np.sqrt(np.mean(np.fft.irfft2(phi.scalar_matrix, s=(256, 256)) ** 2))
+    pairs, pairs_ref = [], []
+    for k in range(16):
+        u = _direction(phi, 4100 + k, "phi")
+        D = lambda e: (lp(phi + u * (e * rms_p)) - lp(phi - u * (e * rms_p))) / (2 * e * rms_p)
+        fd = (4 * D(5e-4) - D(1e-3)) / 3
+        pairs.append((fd, R.dot(gp, u)))
+        pairs_ref.append((fd, R.dot(gp_ref, u)))
+    scale = np.sqrt(np.mean([a * a for a, _ in pairs]))
+    worst = max(abs(a - b) for a, b in pairs) / scale
+    worst_ref = max(abs(a - b) for a, b in pairs_ref) / scale
+    assert worst < 1e-6, (worst, worst_ref)
+    assert worst_ref > 10 * worst  # the reference scheme's RK4 gap is visible at this precision
+
+    S = _problem(Mod, 128, 3.0, "IP", 3.0, 10.0, 14.0, seed=2)
+    So = _as_oracle(S)
+    g32 = grad_phi_logpdf(S["field"], S["phi"], S["data"], S["Cn"], S["Cphi"], S["Cf"], S["M"], S["B"], n=7,
+                          scheme="exact")
+    go = R.grad_phi_logpdf(So["field"], So["phi"], So["data"], So["Cn"], So["Cphi"], So["Cf"], So["M"], So["B"], n=7,
+                           scheme="exact")
+    assert rel_l2(g32.scalar_matrix, go) < 2e-5

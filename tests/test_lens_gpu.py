@@ -46,8 +46,6 @@ def _engine(torch, f, phis, pw, n, direction, adjoint, precision="f32"):
                                        (512, 2.0, 2)])
 @pytest.mark.parametrize("direction,adjoint", [(1, False), (-1, False), (1, True), (-1, True)])
 def test_lens_matches_oracle(torch_cuda, N, theta, C, direction, adjoint):
-    if N == 512 and (direction, adjoint) == (-1, False):
-        pytest.skip("512^2 inverse lens runs the forward kernels with direction -1; covered at smaller N")
     f, phis = _inputs(N, theta, C)
     pw = R.pix_width_of(theta)
     got = _engine(torch_cuda, f, phis, pw, 7, direction, adjoint)[0]
@@ -172,6 +170,60 @@ def test_batch_equals_single(torch_cuda):
     for i in (0, 3):
         one = _engine(torch_cuda, f[i:i + 1], phis[i:i + 1], pw, 7, 1, False)
         assert np.array_equal(one[0], batch[i])
+
+
+@pytest.mark.parametrize("direction,adjoint", [(1, False), (-1, False), (1, True)])
+def test_qu512_batch_maps_equal_solo_and_oracle(torch_cuda, direction, adjoint):
+    """The bench's shape (512^2 QU, p planes, the paired row kernels) at B = 4 distinct maps: every map of the
+    batch is bit-identical to the same map lensed alone (the batch index of k_row_pair / k_row_pair_adj and of
+    k_p_planes), and the last map matches the float64 oracle."""
+    import torch
+    from cmblensing_b200 import engine
+    N, theta, C, B, n = 512, 2.0, 2, 4, 7
+    f, phis = _inputs(N, theta, C, B=B, seed0=40)
+    pw = R.pix_width_of(theta)
+    plan = engine.get_plan(N, C, pw)
+    planes = plan.phi_planes(torch.as_tensor(phis, device="cuda"))
+    ft = torch.as_tensor(f, device="cuda", dtype=torch.float32)
+    ws = torch.empty(plan.workspace_bytes(B, adjoint, n), dtype=torch.uint8, device="cuda")  # the p-plane path
+    batch = plan.lense_flow(ft, planes, n=n, direction=direction, adjoint=adjoint, workspace=ws)
+    for i in range(B):
+        one = plan.lense_flow(ft[i:i + 1], planes[i:i + 1], n=n, direction=direction, adjoint=adjoint)
+        assert torch.equal(one[0], batch[i]), i
+    ref = _oracle(f[B - 1], phis[B - 1], pw, n, direction, adjoint)
+    got = batch[B - 1].double().cpu().numpy()
+    for c in range(C):
+        assert rel_l2(got[c], ref[c]) < TOL32, (c, rel_l2(got[c], ref[c]))
+
+
+def test_lense_flow_backwards_qu_map_phi_matches_oracle(torch_cuda):
+    """The reference-shaped reverse pass on a QU field with a MAP phi and a MAP cotangent: the returned delta-f
+    has Q and U swapped as the reference's output_like_input writes them (lense_flow.py:143-152), and both
+    outputs go through the MAP branch of undo_inner_product (fields.py:147-154) -- against the oracle's
+    lense_flow_backwards.  The reference's default Fourier weights (0.5 on the DC/Nyquist columns) are used."""
+    import cmblensing_b200 as cl
+    from cmblensing_b200.lense_flow import lense_flow_backwards
+    N, theta, n = 128, 3.0, 7
+    f, phis = _inputs(N, theta, 2, seed0=12)
+    pw = R.pix_width_of(theta)
+    rng = np.random.default_rng(13)
+    cot = rng.standard_normal((2, N, N))
+    lensed = _oracle(f[0], phis[0], pw, n, 1, False)
+    kw = dict(nside=N, theta_pix=theta, pix_width=pw)
+    mk = lambda mod, a: mod.FlatS2(polar_matrix_1=a[0], polar_matrix_2=a[1], basis=mod.Basis.MAP, **kw)
+    phi_e = cl.FlatS0(scalar_matrix=phis[0], basis=cl.Basis.MAP, **kw)
+    phi_o = R.FlatS0(scalar_matrix=phis[0], basis=R.Basis.MAP, **kw)
+    df, dphi = lense_flow_backwards(mk(cl, lensed), phi_e, mk(cl, cot), n=n, direction=1)
+    df_o, dphi_o = R.lense_flow_backwards(mk(R, lensed), phi_o, mk(R, cot), n=n, direction=1)
+    assert isinstance(df.polar_matrix_1, np.ndarray) and df.polar_matrix_1.shape == (N, N)
+    # the swap: polar_matrix_1 holds the U component's delta (compare with the unswapped engine output)
+    df_plain, _ = lense_flow_backwards(mk(cl, lensed), phi_e, mk(cl, cot), n=n, direction=1, swap_qu=False)
+    assert np.array_equal(df.polar_matrix_1, df_plain.polar_matrix_2)
+    assert np.array_equal(df.polar_matrix_2, df_plain.polar_matrix_1)
+    assert rel_l2(df.polar_matrix_1, df_o.polar_matrix_1) < 1e-5
+    assert rel_l2(df.polar_matrix_2, df_o.polar_matrix_2) < 1e-5
+    assert dphi.scalar_matrix.shape == (N, N)
+    assert rel_l2(dphi.scalar_matrix, dphi_o.scalar_matrix) < 2e-5
 
 
 def test_round_trip_512_QU(torch_cuda):

@@ -39,27 +39,69 @@ def _call_noalloc(lib, torch, N, C, pw, f, out, planes, B, n, direction, adjoint
                                      B, n, direction, int(adjoint), stream)
 
 
-def test_noalloc_matches_allocating_entry_point_twice(torch_cuda):
+# (N, C, batch, theta): every component count, and twiddle offsets into the shared tables for 64, 256 and 512;
+# the largest needs 5 x 4 x 512^2 x 3 bytes = 15 MiB of the 24 MiB scratch
+SHAPES = [(256, 2, 2, 3.0), (64, 1, 2, 3.0), (512, 3, 1, 2.0)]
+
+
+@pytest.mark.parametrize("N,C,B,theta", SHAPES)
+def test_noalloc_matches_allocating_entry_point_twice(torch_cuda, N, C, B, theta):
     torch = torch_cuda
     from cmblensing_b200 import _native as nat
     from cmblensing_b200 import engine
     from cmblensing_b200.simulate import lens_batch, ARCMIN
     lib = nat.load()
-    N, C, theta = 256, 2, 3.0
     pw = theta * ARCMIN
     plan = engine.get_plan(N, C, pw)
-    # call 1: forward lens of two maps; call 2: adjoint lens of two other maps
+    # call 1: forward lens; call 2: adjoint lens of other maps, on the scratch the first call left behind
     cases = [(0, 1, False), (10, 1, True)]
     for seed0, direction, adjoint in cases:
-        f, phis = lens_batch(N, theta, 2, C, seed0=seed0)
+        f, phis = lens_batch(N, theta, B, C, seed0=seed0)
         ft = torch.as_tensor(f, device="cuda", dtype=torch.float32)
         planes = plan.phi_planes(torch.as_tensor(phis, device="cuda"))
         out = torch.empty_like(ft)
-        status = _call_noalloc(lib, torch, N, C, pw, ft, out, planes, 2, 7, direction, adjoint)
+        status = _call_noalloc(lib, torch, N, C, pw, ft, out, planes, B, 7, direction, adjoint)
         assert status == nat.LF_OK, nat.status_string(status)
         ref = plan.lense_flow(ft, planes, n=7, direction=direction, adjoint=adjoint)
         torch.cuda.synchronize()
         assert rel_l2(out.double().cpu().numpy(), ref.double().cpu().numpy()) < TOL32
+
+
+def test_noalloc_float64_in_place_inverse(torch_cuda):
+    """float64 fields in and out, f_in == f_out (an in-place inverse lens), against the allocating entry point."""
+    torch = torch_cuda
+    from cmblensing_b200 import _native as nat
+    from cmblensing_b200 import engine
+    from cmblensing_b200.simulate import lens_batch, ARCMIN
+    lib = nat.load()
+    N, C, B, theta = 128, 2, 3, 3.0
+    pw = theta * ARCMIN
+    plan = engine.get_plan(N, C, pw)
+    f, phis = lens_batch(N, theta, B, C, seed0=21)
+    planes = plan.phi_planes(torch.as_tensor(phis, device="cuda"))
+    x = torch.as_tensor(f, device="cuda")  # float64
+    ref = plan.lense_flow(x, planes, n=7, direction=-1)
+    for _ in range(2):
+        y = x.clone()
+        status = _call_noalloc(lib, torch, N, C, pw, y, y, planes, B, 7, -1, False)
+        assert status == nat.LF_OK, nat.status_string(status)
+        torch.cuda.synchronize()
+        assert y.dtype == torch.float64
+        assert rel_l2(y.cpu().numpy(), ref.cpu().numpy()) < TOL32
+
+
+def test_noalloc_zero_steps_needs_no_scratch(torch_cuda):
+    """nsteps = 0 returns the input (as lf_lense_flow does), even for a size beyond the scratch."""
+    torch = torch_cuda
+    from cmblensing_b200 import _native as nat
+    lib = nat.load()
+    N, C, B = 1024, 3, 1
+    f = torch.randn((B, C, N, N), device="cuda")
+    out = torch.empty_like(f)
+    planes = torch.zeros((B, 5, N, N), device="cuda")
+    assert _call_noalloc(lib, torch, N, C, 1e-3, f, out, planes, B, 0, 1, False) == nat.LF_OK
+    torch.cuda.synchronize()
+    assert torch.equal(out, f)
 
 
 def test_noalloc_rejects_requests_beyond_its_scratch(torch_cuda):
