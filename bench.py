@@ -52,7 +52,10 @@ def parse():
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-fp64", action="store_true")
     ap.add_argument("--no-e2e", action="store_true")
+    ap.add_argument("--no-workloads", action="store_true", help="skip the gradient and Wiener-filter legs")
     ap.add_argument("--serving-seconds", type=float, default=1.5)
+    ap.add_argument("--serving-requests", type=int, default=2000,
+                    help="requests measured at 80%% of the measured capacity (0: skip that stream)")
     ap.add_argument("--serving-rate", type=float, default=200.0)
     ap.add_argument("--adjoint", action="store_true", help="time the adjoint lens instead of the forward lens")
     return ap.parse_args()
@@ -324,11 +327,159 @@ def _wf_problem(N, C, theta, seed):
     return dict(phi=cl.FlatS0(scalar_matrix=p["phi"], **kw), data=data, Cf=Cf, Cn=Cn, M=mask, B=B)
 
 
-def run_serving(a):
-    """Config-4 stream: Poisson arrivals, mixed kinds/sizes/components; p50/p99 and throughput vs one at a time."""
+def _event_ms(fn, reps=1):
+    """Milliseconds of ``reps`` calls of fn on the current stream (CUDA events, synchronised on both sides)."""
+    import torch
+    torch.cuda.synchronize()
+    e0 = torch.cuda.Event(enable_timing=True)
+    e1 = torch.cuda.Event(enable_timing=True)
+    e0.record()
+    for _ in range(reps):
+        fn()
+    e1.record()
+    torch.cuda.synchronize()
+    return e0.elapsed_time(e1)
+
+
+def run_gradient(a, dev):
+    """Config-2 workload: the LenseFlow part of grad_phi_logpdf at 256^2 IQU, 3' pixels, n = 7, FP32.
+
+    One unit = one (f, phi) pair through the phi-derivative precompute, the
+    forward lens and the reverse pass that yields (delta_f, delta_phi in the
+    Fourier basis), batched 16 pairs per call; the reference scheme (forward
+    lens + reverse ODE from Lf, lf_lense_flow_vjp) and the checkpointed exact
+    scheme (lf_lense_flow_vjp_ckpt, forward included) side by side.
+    """
     import numpy as np
     import torch
-    from cmblensing_b200.serve import Request, Server, latency_summary, run_alone
+    from cmblensing_b200 import engine
+    from cmblensing_b200.simulate import ARCMIN, lens_batch
+    N, C, B, n, theta = 256, 3, 16, 7, 3.0
+    pw = theta * ARCMIN
+    f, phis = lens_batch(N, theta, B, C, seed0=600)
+    plan = engine.get_plan(N, C, pw, "f32", device=dev)
+    ft = torch.as_tensor(f, device=dev, dtype=torch.float32)
+    phif = torch.as_tensor(np.fft.rfft2(phis), device=dev)
+    cot = torch.as_tensor(np.random.default_rng(601).standard_normal(f.shape), device=dev, dtype=torch.float32)
+    planes = torch.empty((B, 5, N, N), dtype=torch.float32, device=dev)
+    phi_ws = torch.empty(plan.phi_workspace_bytes(B), dtype=torch.uint8, device=dev)
+
+    def ref_scheme():
+        plan.phi_planes(phif, check_det=False, out=planes, workspace=phi_ws)
+        lensed = plan.lense_flow(ft, planes, n=n)
+        return plan.lense_flow_vjp(lensed, cot, planes, n=n, phi_basis="fourier")
+
+    def exact_scheme():
+        plan.phi_planes(phif, check_det=False, out=planes, workspace=phi_ws)
+        return plan.lense_flow_vjp_ckpt(ft, cot, planes, n=n, phi_basis="fourier")
+
+    out = {"workload": "grad_lenseflow_iqu256_b16_n7", "nside": N, "ncomp": C, "batch": B, "rk4_steps": n,
+           "theta_pix_arcmin": theta, "unit": "maps/s",
+           "what": "phi precompute + forward lens + reverse pass (delta_f, Fourier delta_phi), FP32"}
+    for name, fn in (("reference_scheme", ref_scheme), ("exact_scheme", exact_scheme)):
+        for _ in range(3):
+            fn()
+        reps = 10
+        ms = _event_ms(fn, reps)
+        out[name] = {"maps_per_s": B * reps / (ms / 1000.0), "ms_per_call": ms / reps}
+    _, dphi_r = ref_scheme()
+    _, dphi_e = exact_scheme()
+    torch.cuda.synchronize()
+    out["rel_l2_exact_vs_reference_dphi"] = float((dphi_e - dphi_r).norm() / dphi_r.norm())
+    out["note"] = ("the two schemes' delta-phi differ by the reference scheme's RK4 discretisation gap; "
+                   "tests/test_configs_gpu.py checks the exact one against finite differences to 1e-6")
+    return out
+
+
+def run_wf(a, dev):
+    """Config-3 workload: lensed Wiener filter at 512^2 QU, 2' pixels, 1' beam, 2 uK' pol noise, 30-hole mask.
+
+    A batch of 8 problems solved together by the device PCG (FP32 operator,
+    float64 dots, true residual from the FP64 engine every 10 iterations,
+    CG blocks replayed from a CUDA graph) to ||r||/||b|| = 1e-6; one
+    application of A for the batch timed alone; problem 0 solved again by the
+    FP64 engine to 1e-10 as the reference solution.
+    """
+    import torch
+    from cmblensing_b200.wf_engine import DeviceWienerFilter
+    N, C, theta, B = 512, 2, 2.0, 8
+    probs = [_wf_problem(N, C, theta, seed=700 + i) for i in range(B)]
+    wf = DeviceWienerFilter(problems=probs, n=7)
+    x0 = wf.b_vector()
+    for _ in range(3):
+        wf.apply_A(x0)
+    reps = []
+    for _ in range(9):
+        reps.append(_event_ms(lambda: wf.apply_A(x0)))
+    a_ms = sorted(reps)[len(reps) // 2]
+    wf64 = DeviceWienerFilter(problems=probs[:1], n=7, precision="f64")
+    x64, it64 = wf64.solve(rel_tol=1e-10, maxiter=3000)
+    out = {"workload": "wf_qu512_masked_b8_n7", "nside": N, "ncomp": C, "batch": B, "rk4_steps": 7,
+           "theta_pix_arcmin": theta, "beam_fwhm_arcmin": 1.0, "noise_pol_uk_arcmin": 2.0, "mask": "30 holes",
+           "refine_every": 10, "apply_A_ms_batch": a_ms, "apply_A_ms_per_problem": a_ms / B,
+           "fp64_solution": {"rel_tol": 1e-10, "iterations": it64, "engine": "FP64 operator"}}
+    # to the workload's 1e-6 relative residual, and further, to a solution within 1e-6 of the FP64 one
+    for key, tol in (("solve_rel_tol_1e-6", 1e-6), ("solve_rel_tol_1e-8", 1e-8)):
+        kw = dict(rel_tol=tol, refine_every=10, maxiter=1000)
+        wf.solve(**kw)  # warm: plans, graph capture path
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        x, its = wf.solve(**kw)
+        torch.cuda.synchronize()
+        wall = time.perf_counter() - t0
+        out[key] = {"iterations": its, "solve_wall_s_batch": wall, "wall_s_per_solve": wall / B,
+                    "graph_blocks_replayed": wf.graph_blocks,
+                    "rel_l2_vs_fp64_solution": float((x[0] - x64).norm() / x64.norm())}
+    return out
+
+
+def _serve_stream(srv, make, rng, rate, nreq, warm=0):
+    """Submit ``warm + nreq`` requests as a Poisson stream at ``rate`` (None: all at once), wait for all;
+    return (the ``nreq`` measured requests, seconds from the first measured submission to the last
+    completion)."""
+    import numpy as np
+    reqs = [make() for _ in range(warm + nreq)]
+    gaps = rng.exponential(1.0 / rate, size=len(reqs)) if rate else np.zeros(len(reqs))
+    tnext = time.perf_counter()
+    for r, g in zip(reqs, gaps):
+        tnext += g
+        dt = tnext - time.perf_counter()
+        if dt > 0:
+            time.sleep(dt)
+        srv.submit(r)
+    t_wait = time.perf_counter()
+    ok = all(r.done.wait(max(1.0, 900 - (time.perf_counter() - t_wait))) for r in reqs)
+    meas = reqs[warm:]
+    t_end = max((r.t_done for r in meas if r.t_done), default=time.perf_counter())
+    return meas, t_end - meas[0].t_submit, ok
+
+
+def _serve_summary(reqs, span, ok):
+    from cmblensing_b200.serve import latency_summary
+    wsum = sum(r.nside * r.nside * r.ncomp for r in reqs if r.error is None) / (512.0 * 512.0 * 2)
+    lat = [r for r in reqs if r.latency is not None]
+    k = max(1, len(lat) // 10)
+    return {"requests": len(reqs), "all_completed": bool(ok), "errors": sum(r.error is not None for r in reqs),
+            "error_samples": sorted({f"{r.kind} N={r.nside} C={r.ncomp}: {r.error!r}"[:300]
+                                     for r in reqs if r.error})[:4],
+            "seconds": span, "requests_per_s": len(reqs) / span,
+            "qu512_equivalent_maps_per_s": wsum / span,
+            "latency": latency_summary(reqs),
+            "latency_by_kind": {kd: latency_summary([r for r in reqs if r.kind == kd])
+                                for kd in ("lens", "delens", "wf")},
+            # a bounded queue: the last tenth of the stream waits no longer than the first
+            "p50_first_tenth_ms": latency_summary(lat[:k]).get("p50_ms"),
+            "p50_last_tenth_ms": latency_summary(lat[-k:]).get("p50_ms")}
+
+
+def run_serving(a):
+    """Config-4 stream: mixed kinds/sizes/components.  (1) capacity: a burst of requests submitted at once,
+    completions per second; (2) a Poisson stream at 80% of that capacity, ``--serving-requests`` measured
+    after a tenth as many warm-up requests; (3) the specified 200 req/s for ``--serving-seconds``; and the same
+    mix one request at a time with plain engine calls."""
+    import numpy as np
+    import torch
+    from cmblensing_b200.serve import Request, Server, run_alone
     from cmblensing_b200.simulate import lens_batch
     rng = np.random.default_rng(4242)
     pools, wf = {}, {}
@@ -358,39 +509,33 @@ def run_serving(a):
              for N, th in SERVE_SIZES.items() for C in (1, 2)]
     for r in warm:
         r.done.wait(300)
-    srv.completed.clear()
-    # the stream
+    out = {"mix": "50% lens / 20% inverse / 30% Wiener filter; N 128/256/512/1024 at 0.4/0.3/0.2/0.1; "
+                  "T or QU 50/50", "wf_stop": "||r||/||b|| < 1e-5, FP64 residual every 10 iterations",
+           "weighting": "qu512_equivalent_maps_per_s counts a request as N^2 C / (512^2 * 2) maps"}
+    burst, span, ok = _serve_stream(srv, make, rng, None, max(60, a.serving_requests // 8))
+    cap = len(burst) / span
+    out["capacity"] = {"requests_per_s": cap, "method": "a burst submitted at once, completions per second",
+                       **{k: v for k, v in _serve_summary(burst, span, ok).items() if k != "latency_by_kind"}}
+    if a.serving_requests > 0:
+        reqs, span, ok = _serve_stream(srv, make, rng, 0.8 * cap, a.serving_requests,
+                                       warm=max(1, a.serving_requests // 10))
+        out["at_80pct_capacity"] = {"offered_per_s": 0.8 * cap, **_serve_summary(reqs, span, ok)}
     nreq = int(rng.poisson(a.serving_rate * a.serving_seconds))
-    gaps = rng.exponential(1.0 / a.serving_rate, size=nreq)
-    reqs = [make() for _ in range(nreq)]
-    t0 = time.perf_counter()
-    tnext = t0
-    for r, g in zip(reqs, gaps):
-        tnext += g
-        dt = tnext - time.perf_counter()
-        if dt > 0:
-            time.sleep(dt)
-        srv.submit(r)
-    ok = all(r.done.wait(max(1.0, 600 - (time.perf_counter() - t0))) for r in reqs)
-    t_end = max((r.t_done for r in reqs if r.t_done), default=time.perf_counter())
+    if nreq > 0:
+        reqs, span, ok = _serve_stream(srv, make, rng, a.serving_rate, nreq)
+        out["at_specified_rate"] = {"offered_per_s": a.serving_rate, "seconds_of_arrivals": a.serving_seconds,
+                                    **_serve_summary(reqs, span, ok)}
     srv.stop()
-    errors = sum(r.error is not None for r in reqs)
-    span = t_end - t0
-    out = {"requests": nreq, "arrival_rate_per_s": a.serving_rate, "seconds_of_arrivals": a.serving_seconds,
-           "all_completed": bool(ok), "errors": errors, "throughput_maps_per_s": nreq / span,
-           "latency": latency_summary(reqs),
-           "latency_by_kind": {k: latency_summary([r for r in reqs if r.kind == k]) for k in ("lens", "delens", "wf")},
-           "mix": "50% lens / 20% inverse / 30% Wiener filter; N 128/256/512/1024 at 0.4/0.3/0.2/0.1; T or QU 50/50"}
     # one request at a time, plain engine calls, on a sample of the same mix
-    sample = reqs[: min(len(reqs), 40)]
+    sample = [make() for _ in range(40)]
     torch.cuda.synchronize()
     ts = time.perf_counter()
     for r in sample:
         run_alone(r)
     torch.cuda.synchronize()
-    seq = (time.perf_counter() - ts) / max(len(sample), 1)
-    out["one_at_a_time"] = {"maps_per_s": 1.0 / seq, "sample_requests": len(sample)}
-    out["speedup_vs_one_at_a_time"] = out["throughput_maps_per_s"] * seq
+    seq = (time.perf_counter() - ts) / len(sample)
+    out["one_at_a_time"] = {"requests_per_s": 1.0 / seq, "sample_requests": len(sample)}
+    out["capacity_over_one_at_a_time"] = cap * seq
     return out
 
 # --------------------------------------------------------------------- main
@@ -559,19 +704,35 @@ def main():
         p64 = torch.as_tensor(phi_host[:nb], device=dev)
         lense_flow_fp64(f64, p64, pw, n)
         torch.cuda.synchronize()
-        t0 = time.perf_counter()
-        ref64 = lense_flow_fp64(f64, p64, pw, n)
-        torch.cuda.synchronize()
-        dt = time.perf_counter() - t0
+        reps = []
+        for _ in range(7):  # the median of seven event-timed calls
+            c0 = torch.cuda.Event(enable_timing=True)
+            c1 = torch.cuda.Event(enable_timing=True)
+            c0.record()
+            ref64 = lense_flow_fp64(f64, p64, pw, n)
+            c1.record()
+            torch.cuda.synchronize()
+            reps.append(c0.elapsed_time(c1) / 1000.0)
+        dt = sorted(reps)[len(reps) // 2]
         ours = out_dev[:nb].double()
         rel = float((ours - ref64).norm() / ref64.norm())
-        result["fp64_restatement"] = {"value": nb / dt, "unit": UNIT, "batch": nb,
+        result["fp64_restatement"] = {"value": nb / dt, "unit": UNIT, "batch": nb, "repeats": len(reps),
+                                      "spread_s": [min(reps), max(reps)],
                                       "what": "torch float64 restatement of the reference op sequence (cuFFT), "
-                                              "not the reference", "speedup_of_value": value / world / (nb / dt),
+                                              "not the reference; median of 7 CUDA-event-timed calls",
+                                      "speedup_of_value": value / world / (nb / dt),
                                       "rel_l2_fp32_vs_fp64": rel}
 
+    # ---------------------------------------------------- configs 2 and 3
+    if rank == 0 and not a.no_workloads:
+        for key, fn in (("gradient", run_gradient), ("wf", run_wf)):
+            try:
+                result[key] = fn(a, dev)
+            except Exception as e:  # the headline numbers stand on their own
+                result[key] = {"error": repr(e)}
+
     # ---------------------------------------------------- serving
-    if rank == 0 and a.serving_seconds > 0:
+    if rank == 0 and (a.serving_seconds > 0 or a.serving_requests > 0):
         try:
             result["serving"] = run_serving(a)
         except Exception as e:  # the headline numbers stand on their own

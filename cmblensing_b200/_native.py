@@ -54,6 +54,8 @@ SIGNATURES = {
     "lf_lense_flow_vjp": (_i, [_vp, _vp, _vp, _i, _vp, _i, _i, _i, _vp, _vp, _vp, _i, _vp, _sz, _vp]),
     "lf_vjp_ckpt_workspace_bytes": (_sz, [_vp, _i, _i]),
     "lf_lense_flow_vjp_ckpt": (_i, [_vp, _vp, _vp, _i, _vp, _i, _i, _i, _vp, _vp, _vp, _i, _vp, _sz, _vp]),
+    "lf_modes_apply": (_i, [_vp, _i, ctypes.c_uint, _vp, _vp, _vp, _i, _i, ctypes.c_long, ctypes.c_double,
+                            ctypes.c_double, _vp]),
     "lf_lense_flow_noalloc": (_i, [_i, _i, ctypes.c_double, _vp, _i, _vp, _i, _vp, _i, _i, _i, _i, _vp]),
     "lf_profile_enable": (_i, [_vp, _i]),
     "lf_profile_reset": (_i, [_vp]),

@@ -1127,6 +1127,27 @@ int lf_lense_flow_vjp_ckpt(lf_plan_t p, const void* f_in, const void* cotangent,
   return cuda_status(finish_dphi(p->N, batch, dacc, spec, dphi_f, dphi, dphi_basis, p->tw64, af.kbase, st));
 }
 
+int lf_modes_apply(const void* W, int w_batched, unsigned nonzero, const void* X, const void* Y, void* out, int batch,
+                   int ncomp, long modes, double scale, double yscale, void* stream) {
+  if (batch < 0 || modes < 0 || ncomp < 1 || ncomp > 3) return LF_ERR_BAD_SHAPE;
+  if (batch == 0 || modes == 0) return LF_OK;
+  if (!W || !X || !out || !aligned16(X) || !aligned16(out) || (Y && !aligned16(Y))) return LF_ERR_BAD_ARG;
+  if (reinterpret_cast<uintptr_t>(W) & 7u) return LF_ERR_BAD_ARG;
+  const long total = (long)batch * modes;
+  const dim3 grid((unsigned)std::min<long>((total + 255) / 256, 148L * 16));
+  cudaStream_t st = (cudaStream_t)stream;
+  const double* w = static_cast<const double*>(W);
+  const double2* x = static_cast<const double2*>(X);
+  const double2* y = static_cast<const double2*>(Y);
+  double2* o = static_cast<double2*>(out);
+  cudaError_t e;
+  g_prof = nullptr;
+  if (ncomp == 1) e = launch<k_modes_apply<1>>(grid, 256, 0, st, w, w_batched, nonzero, x, y, o, batch, modes, scale, yscale);
+  else if (ncomp == 2) e = launch<k_modes_apply<2>>(grid, 256, 0, st, w, w_batched, nonzero, x, y, o, batch, modes, scale, yscale);
+  else e = launch<k_modes_apply<3>>(grid, 256, 0, st, w, w_batched, nonzero, x, y, o, batch, modes, scale, yscale);
+  return cuda_status(e);
+}
+
 int lf_profile_enable(lf_plan_t p, int enable) {
   if (!p) return LF_ERR_BAD_ARG;
   p->prof.on = enable != 0;

@@ -1190,3 +1190,50 @@ __global__ void __launch_bounds__(NT) k_spec_cols_inv(const double2* __restrict_
 }
 
 }  // namespace lf
+
+namespace lf {
+
+// ================================================ per-mode operator products
+// out[b][i][m] = s * sum_j W[b or 0][i][j][m] * X[b][j][m] + t * Y[b][i][m]
+// for the Fourier-diagonal C x C operators of the Wiener filter
+// (matrix_operators.py:54-141, the EB<->QU rotation of util.py:140-161):
+// W real float64 [Bw][C][C][M] (Bw = 1 broadcasts), X / Y / out complex128
+// [B][C][M].  Bit (i C + j) of ``nz`` marks the blocks that are not
+// identically zero; the others are neither read nor multiplied.  Every
+// output of a mode is formed from registers before any is stored, so out may
+// alias X or Y.
+template <int C>
+__global__ void __launch_bounds__(256) k_modes_apply(const double* __restrict__ W, int w_batched, unsigned nz,
+                                                     const double2* X, const double2* Y, double2* out, int B, long M,
+                                                     double s, double t) {
+  const long total = (long)B * M;
+  for (long e = blockIdx.x * (long)blockDim.x + threadIdx.x; e < total; e += (long)gridDim.x * blockDim.x) {
+    const long b = e / M, m = e % M;
+    const double* w = W + (w_batched ? b : 0) * (long)C * C * M + m;
+    double2 x[C], o[C];
+#pragma unroll
+    for (int j = 0; j < C; ++j) x[j] = X[(b * C + j) * M + m];
+#pragma unroll
+    for (int i = 0; i < C; ++i) {
+      double re = 0.0, im = 0.0;
+#pragma unroll
+      for (int j = 0; j < C; ++j) {
+        if (nz & (1u << (i * C + j))) {
+          const double wij = w[(long)(i * C + j) * M];
+          re += wij * x[j].x;
+          im += wij * x[j].y;
+        }
+      }
+      o[i] = make_double2(s * re, s * im);
+      if (Y) {
+        const double2 y = Y[(b * C + i) * M + m];
+        o[i].x += t * y.x;
+        o[i].y += t * y.y;
+      }
+    }
+#pragma unroll
+    for (int i = 0; i < C; ++i) out[(b * C + i) * M + m] = o[i];
+  }
+}
+
+}  // namespace lf

@@ -286,7 +286,7 @@ class HostPipeline:
     With ``use_graphs`` each chunk's phi precompute + lens (about 60 launches)
     is captured into a CUDA graph at the second call of a given shape (the
     first runs eagerly, which also sets the kernels' shared-memory limits) and
-    replayed from then on; the capture synchronises the device once.  For 64
+    replayed from then on (captured without a device-wide synchronisation).  For 64
     512^2 QU maps with float64 host I/O: 4,528 maps/s on one stream, 5,600
     with two compute streams, 6,411 with graphs, 7,240 with consecutive calls
     queued (``wait=False``) so that each call's fill and drain overlap its
@@ -434,10 +434,8 @@ class HostPipeline:
                 key = (i,) + args[2:]
                 g = self.graphs.get(key) if self.use_graphs else None
                 if g is None and self.use_graphs and key in self._warm:
-                    # thread-local capture: the copy streams keep running meanwhile
-                    g = torch.cuda.CUDAGraph()
-                    with torch.cuda.graph(g, stream=sc, capture_error_mode="thread_local"):
-                        self._compute(*args)
+                    # thread-local capture on the compute stream: the copy streams keep running meanwhile
+                    g = capture_graph(lambda: self._compute(*args), stream=sc)
                     self.graphs[key] = g
                 if g is not None:
                     g.replay()
@@ -514,6 +512,32 @@ class LenseFlowFunction(torch.autograd.Function):
 def lense_flow_ad(f, phi, pix_width, n=10, direction=FORWARD_LENSE, precision="f32", scheme="reference"):
     """Differentiable LenseFlow (torch autograd) on device tensors; ``scheme`` selects the reverse pass."""
     return LenseFlowFunction.apply(f, phi, pix_width, n, direction, precision, scheme)
+
+
+def capture_graph(fn, stream=None):
+    """Capture the launches of ``fn()`` into a CUDA graph on ``stream`` without synchronising the device.
+
+    ``torch.cuda.graph`` synchronises the whole device and empties the
+    allocator's cache before it begins; while another host thread is
+    capturing, that synchronisation is an illegal operation on the capturing
+    stream and invalidates its capture.  Here the capture begins on the
+    given (non-default) stream directly, in thread-local mode, so threads
+    that capture concurrently -- a server's lens slots and its Wiener-filter
+    workers -- leave one another alone.  With ``stream`` None the current
+    stream is used unless it is the default stream, in which case a side
+    stream is.  Replay the returned graph on any stream."""
+    dev = torch.cuda.current_device()
+    if stream is None:
+        cur = torch.cuda.current_stream(dev)
+        stream = cur if cur != torch.cuda.default_stream(dev) else torch.cuda.Stream(dev)
+    g = torch.cuda.CUDAGraph()
+    with torch.cuda.stream(stream):
+        g.capture_begin(capture_error_mode="thread_local")
+        try:
+            fn()
+        finally:
+            g.capture_end()
+    return g
 
 
 def wait_timeouts(reset=False):

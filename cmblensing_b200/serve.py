@@ -135,10 +135,9 @@ class _LensSlot:
                 g = self.graphs.get(bb)
                 if g is None:
                     self._body(bb)  # eager warm-up: kernel attributes are set outside the capture
-                    g = torch.cuda.CUDAGraph()
-                    # thread-local capture: Wiener-filter workers keep running on their own threads
-                    with torch.cuda.graph(g, stream=self.stream, capture_error_mode="thread_local"):
-                        self._body(bb)
+                    # thread-local capture without a device-wide synchronisation: Wiener-filter
+                    # workers keep running, and capturing, on their own threads
+                    g = engine.capture_graph(lambda: self._body(bb), stream=self.stream)
                     self.graphs[bb] = g
                 g.replay()
             else:

@@ -12,19 +12,26 @@ application of A f = gradf_logpdf(f, d = 0) is
     z  = rfft2(L^T irfft2(h))                    L^T: adjoint LenseFlow
     Ax = -(R z + Cf^-1 x)
 
-with the FFTs and lensing on the engine's kernels, the phi derivatives
-computed once, the CG scalars kept on the device (no host round trip per
-iteration) and one host synchronisation per convergence check.  Optional
-true-residual replacement every ``refine_every`` iterations uses the FP64
-engine for b - A x.
+The per-mode products run in one fused kernel each (lf_modes_apply: real
+float64 matrices, blocks that are zero everywhere skipped), the FFTs on the
+engine's float64 kernels, and the maps between the FFTs and the lens are
+float32 for the FP32 operator (float64 for the FP64 operator of the
+true-residual refinement).  The CG keeps every vector and scalar on the
+device; a problem that has converged is masked on the device (alpha =
+beta = 0), so a block of iterations needs no host decision and is captured
+once as a CUDA graph and replayed: the host synchronises once per block,
+not once per iteration.  Optional true-residual replacement every
+``refine_every`` iterations uses the FP64 engine for b - A x.
 """
 from __future__ import annotations
 
+import ctypes
 import math
 
 import numpy as np
 import torch
 
+from . import _native as nat
 from . import engine
 from ._device import device, to_device
 from .fields import FlatS0, FlatS02, FlatS2, _eb_angle, map as to_map
@@ -61,6 +68,14 @@ def _op_matrix(op, C, like):
 def _mm(A, B):
     """Per-mode matrix product of (C, C, N, H) matrices."""
     return torch.einsum("ijnh,jknh->iknh", A, B)
+
+
+def _nonzero_mask(W):
+    """Bit i*C+j set where block (i, j) of the per-mode operator W ((B,)C,C,N,H) is not identically zero."""
+    Wb = W if W.dim() == 5 else W.unsqueeze(0)
+    C = Wb.shape[1]
+    nz = (Wb != 0).flatten(3).any(dim=3).any(dim=0).cpu().tolist()
+    return sum(1 << (i * C + j) for i in range(C) for j in range(C) if nz[i][j])
 
 
 class DeviceWienerFilter:
@@ -119,27 +134,36 @@ class DeviceWienerFilter:
         kinds = {m is None for m in masks}
         if len(kinds) != 1:
             raise ValueError("a batch mixes map-space and Fourier-diagonal masks")
-        cx = lambda lst: torch.stack(lst).to(torch.complex128)
-        self.R_c = R.to(torch.complex128)          # identical for the batch (same N, pixel size)
-        self.RT_c = RT.to(torch.complex128)
-        self.Cf_inv = cx(Cfi)
-        self.P_inv = cx(Pinv)
+        # per-mode operators as real float64 (C, C, N, H) (shared) or (B, C, C, N, H) (per problem)
+        st = lambda lst: torch.stack(lst).to(torch.float64).contiguous()
+        self.R_c = R.to(torch.float64).contiguous()          # identical for the batch (same N, pixel size)
+        self.RT_c = RT.to(torch.float64).contiguous()
+        self.Cf_inv = st(Cfi)
+        self.P_inv = st(Pinv)
         self.weights = torch.stack(weights)[:, None, None, :]  # (B, 1, 1, N/2+1)
         self.pixel_mask = None
         if masks[0] is not None:
-            self.pixel_mask = torch.stack(masks)[:, None]         # (B, 1, N, N)
-            self.W_b, self.W_n = cx(Wb), cx(Wn)
-            self._b_rt_cn = cx([b[0] for b in bparts])
-            self._b_bm_r = cx([b[1] for b in bparts])
+            pm = torch.stack(masks)[:, None]                     # (B, 1, N, N)
+            self.pixel_mask = {"f64": pm.to(torch.float64), "f32": pm.to(torch.float32)}
+            self.W_b, self.W_n = st(Wb), st(Wn)
+            self._b_rt_cn = st([b[0] for b in bparts])
+            self._b_bm_r = st([b[1] for b in bparts])
         else:
-            self.W_data, self._bm_cn = cx(Wd), cx(Bc)
+            self.W_data, self._bm_cn = st(Wd), st(Bc)
         self.d = torch.stack([torch.stack([getattr(dd, k) for k in dd._matrix_names()]) for dd in self.datas])
         self.phimap = torch.stack(phis)
         self.plan = engine.get_plan(N, C, self.pw, precision, device=dev)
         self.planes = engine.cached_phi_planes(self.plan, self.phimap)
         self.fft = engine.get_plan(N, 1, self.pw, "f64", device=dev)
         self._plan64 = None
-        self._nonzero = {}  # per-mode operator -> which of its C x C blocks are not identically zero
+        self._lib = self.plan._lib
+        # which C x C blocks of every per-mode operator are not identically zero (found once, here)
+        self._nonzero = {}
+        for W in [self.R_c, self.RT_c, self.Cf_inv, self.P_inv] + (
+                [self.W_b, self.W_n, self._b_rt_cn, self._b_bm_r] if self.pixel_mask is not None
+                else [self.W_data, self._bm_cn]):
+            self._nonzero[(W.data_ptr(), tuple(W.shape))] = _nonzero_mask(W)
+        self.graph_blocks = 0  # CG blocks replayed from a captured graph in the last solve
 
     # ----------------------------------------------------------- pieces
     @staticmethod
@@ -175,35 +199,27 @@ class DeviceWienerFilter:
             out[2, 2] = rec(P[2, 2])
         return out
 
-    def _apply(self, W, X):
-        """Per-mode matrix times vector: W (C,C,N,H) shared or (B,C,C,N,H) per problem; X (B,C,N,H).
-
-        Written as C x C elementwise products (memory-bound, one pass each)
-        rather than an einsum, and skipping the blocks of W that are zero
-        everywhere (an EB-diagonal operator has no off-diagonal blocks); which
-        blocks those are is found once per operator."""
-        Wb = W if W.dim() == 5 else W.unsqueeze(0)
-        C = Wb.shape[1]
-        key = (W.data_ptr(), tuple(W.shape))
-        nz = self._nonzero.get(key)
-        if nz is None:
-            nz = [[bool(torch.any(Wb[:, i, j] != 0)) for j in range(C)] for i in range(C)]
-            self._nonzero[key] = nz
-        out = torch.empty(X.shape, dtype=torch.result_type(Wb, X), device=X.device)
-        for i in range(C):
-            terms = [j for j in range(C) if nz[i][j]]
-            if not terms:
-                out[:, i] = 0
-                continue
-            acc = Wb[:, i, terms[0]] * X[:, terms[0]]
-            for j in terms[1:]:
-                acc = acc + Wb[:, i, j] * X[:, j]
-            out[:, i] = acc
+    def _apply(self, W, X, scale=1.0, Y=None, yscale=0.0):
+        """scale * (W X) + yscale * Y per mode: W (C,C,N,H) shared or (B,C,C,N,H) per problem (real float64);
+        X, Y (B,C,N,H) complex128.  One fused kernel (lf_modes_apply)."""
+        B, C = X.shape[0], X.shape[1]
+        X = X.contiguous()
+        out = torch.empty(X.shape, dtype=torch.complex128, device=X.device)
+        nz = self._nonzero[(W.data_ptr(), tuple(W.shape))]
+        st = ctypes.c_void_p(torch.cuda.current_stream(X.device).cuda_stream)
+        nat.check(self._lib.lf_modes_apply(ctypes.c_void_p(W.data_ptr()), int(W.dim() == 5), nz,
+                                           ctypes.c_void_p(X.data_ptr()),
+                                           ctypes.c_void_p(Y.contiguous().data_ptr()) if Y is not None else None,
+                                           ctypes.c_void_p(out.data_ptr()), B, C, X.shape[2] * X.shape[3],
+                                           float(scale), float(yscale), st), "lf_modes_apply")
         return out
 
-    def _irfft2(self, X):
+    def _irfft2(self, X, prec="f64"):
+        """irfft2 of (B, C, N, H) spectra into float64 maps, or float32 maps for the FP32 operator."""
         B, C = X.shape[:2]
-        return self.fft.irfft2(X.reshape(B * C, self.N, self.N // 2 + 1)).reshape(B, C, self.N, self.N)
+        dt = torch.float32 if prec == "f32" else torch.float64
+        return self.fft.irfft2(X.reshape(B * C, self.N, self.N // 2 + 1), out_dtype=dt).reshape(B, C, self.N,
+                                                                                                 self.N)
 
     def _rfft2(self, X):
         B, C = X.shape[:2]
@@ -219,13 +235,13 @@ class DeviceWienerFilter:
             plan, planes = self._plan64, self._planes64
         return plan.lense_flow(q, planes, n=self.n, adjoint=adjoint)
 
-    def _mask_chain(self, y):
-        """QU spectra -> W y through the map-space mask: B, m, Cn^-1, m, B."""
-        m = self.pixel_mask
+    def _mask_chain(self, y, prec):
+        """QU spectra -> W y through the map-space mask: B, m, Cn^-1, m, B (maps in the operator's precision)."""
+        m = self.pixel_mask[prec]
         t = self._apply(self.W_b, y)
-        t = self._rfft2(self._irfft2(t) * m)
+        t = self._rfft2(self._irfft2(t, prec) * m)
         t = self._apply(self.W_n, t)
-        t = self._rfft2(self._irfft2(t) * m)
+        t = self._rfft2(self._irfft2(t, prec) * m)
         return self._apply(self.W_b, t)
 
     def apply_A(self, x, prec=None):
@@ -234,72 +250,117 @@ class DeviceWienerFilter:
         if single:
             x = x.unsqueeze(0)
         prec = prec or self.precision
-        y = self._rfft2(self._lens(self._irfft2(self._apply(self.RT_c, x)), False, prec))
-        h = self._mask_chain(y) if self.pixel_mask is not None else self._apply(self.W_data, y)
-        z = self._rfft2(self._lens(self._irfft2(h), True, prec))
-        out = -(self._apply(self.R_c, z) + self._apply(self.Cf_inv, x))
+        y = self._rfft2(self._lens(self._irfft2(self._apply(self.RT_c, x), prec), False, prec))
+        h = self._mask_chain(y, prec) if self.pixel_mask is not None else self._apply(self.W_data, y)
+        z = self._rfft2(self._lens(self._irfft2(h, prec), True, prec))
+        out = self._apply(self.Cf_inv, x, -1.0, self._apply(self.R_c, z), -1.0)  # -(R z + Cf^-1 x)
         return out[0] if single else out
 
     def b_vector(self, prec=None):
         """b = -gradf_logpdf(0, d) (wiener_filter.py:29-33), (B, C, N, N/2+1)."""
         prec = prec or self.precision
         if self.pixel_mask is not None:
-            t = self._rfft2(self._irfft2(self._apply(self._b_rt_cn, self.d)) * self.pixel_mask)
+            t = self._rfft2(self._irfft2(self._apply(self._b_rt_cn, self.d)) * self.pixel_mask["f64"])
             h = self._apply(self.RT_c, self._apply(self._b_bm_r, t))
         else:
             h = self._apply(self.RT_c, self._apply(self._bm_cn, self.d))
-        z = self._rfft2(self._lens(self._irfft2(h), True, prec))
-        return -self._apply(self.R_c, z)
+        z = self._rfft2(self._lens(self._irfft2(h, prec), True, prec))
+        return self._apply(self.R_c, z, -1.0)
 
     def dot(self, a, b):
         """fields.dot per problem: Re sum conj(a) b w / N^2, float64 device tensor of shape (B,)."""
         return torch.real(torch.sum(torch.conj(a) * b * self.weights, dim=(1, 2, 3))) / (self.N * self.N)
 
     # ------------------------------------------------------------ solve
-    def solve(self, x0=None, rel_tol=None, tol=1e-1, maxiter=500, refine_every=0, check_every=1, history=None):
+    def _iteration(self, S, refine):
+        """One PCG iteration of the reference recurrence on the device state S (updated in place).
+
+        Inactive problems get alpha = beta = 0 (their iterate stays), and the
+        stopping rule is evaluated on the device at the end of the iteration,
+        so a block of iterations needs no host decision."""
+        bc = lambda v: v[:, None, None, None]
+        active = S["active"]
+        Ap = self.apply_A(S["p"])
+        pAp = self.dot(S["p"], Ap)
+        alpha = torch.where(active, S["res"] / torch.where(pAp != 0, pAp, torch.ones_like(pAp)),
+                            torch.zeros_like(pAp))
+        S["x"].add_(bc(alpha) * S["p"])
+        S["iters"].add_(active.to(torch.int64))
+        if refine:  # true residual with the FP64 engine (residual replacement)
+            S["r"].copy_(torch.where(bc(active), S["b"] - self.apply_A(S["x"], "f64"), S["r"]))
+        else:
+            S["r"].sub_(bc(alpha) * Ap)
+        z = self._apply(self.P_inv, S["r"])
+        res_new = self.dot(S["r"], z)
+        beta = torch.where(active, res_new / torch.where(S["res"] != 0, S["res"], torch.ones_like(res_new)),
+                           torch.zeros_like(res_new))
+        S["p"].copy_(z + bc(beta) * S["p"])
+        S["res"].copy_(torch.where(active, res_new, S["res"]))
+        self._update_active(S)
+
+    def _update_active(self, S):
+        """Stopping rule per problem (wiener_filter.py:75-77: r.z < tol; or ||r|| / ||b|| < rel_tol)."""
+        if S["rel_tol"] is None:
+            S["active"].logical_and_(S["res"] >= S["tol"])
+        else:
+            rn = torch.sqrt(torch.clamp(self.dot(S["r"], S["r"]), min=0.0)) / S["bnorm"]
+            S["rn"].copy_(rn)
+            S["active"].logical_and_(~(rn < S["rel_tol"]))
+
+    def solve(self, x0=None, rel_tol=None, tol=1e-1, maxiter=500, refine_every=0, check_every=10, history=None,
+              use_graphs=True):
         """PCG with the reference recurrence for every problem; returns (x, iterations) for a batch of one,
         else (x [B, C, N, N/2+1], iterations per problem).  Stopping per problem as wiener_filter.py:75-77
-        (r.z < tol) unless ``rel_tol`` is given (||r|| / ||b||)."""
+        (r.z < tol) unless ``rel_tol`` is given (||r|| / ||b||).
+
+        Iterations run in blocks of ``refine_every`` (else ``check_every``);
+        the host reads whether any problem is still active once per block.
+        With ``use_graphs`` the first block runs eagerly (kernel attributes,
+        the FP64 refinement plan), the second is captured as a CUDA graph, and
+        every later full block replays it.  The iteration counts per problem
+        equal those of a per-iteration check (the stopping rule is applied on
+        the device every iteration); ``history`` (per-iteration ||r||/||b||)
+        forces eager blocks of one iteration."""
         b = self.b_vector()
-        x = torch.zeros_like(b) if x0 is None else (x0 if x0.dim() == 4 else x0.unsqueeze(0))
+        x = torch.zeros_like(b) if x0 is None else (x0 if x0.dim() == 4 else x0.unsqueeze(0)).clone()
         r = b - self.apply_A(x) if x0 is not None else b.clone()
         z = self._apply(self.P_inv, r)
-        p = z.clone()
-        res = self.dot(r, z)
-        bnorm = torch.sqrt(self.dot(b, b))
-        active = torch.ones(self.batch, dtype=torch.bool, device=self.dev)
-        iters = torch.zeros(self.batch, dtype=torch.int64, device=self.dev)
+        S = {"b": b, "x": x, "r": r, "p": z.clone(), "res": self.dot(r, z),
+             "bnorm": torch.sqrt(self.dot(b, b)), "rel_tol": rel_tol, "tol": tol,
+             "active": torch.ones(self.batch, dtype=torch.bool, device=self.dev),
+             "iters": torch.zeros(self.batch, dtype=torch.int64, device=self.dev),
+             "rn": torch.zeros(self.batch, dtype=torch.float64, device=self.dev)}
+        self._update_active(S)
+        k = int(refine_every) if refine_every else max(1, int(check_every))
+        if history is not None:
+            k, use_graphs = 1, False
         it = 0
-        bc = lambda v: v[:, None, None, None]
+        graph = None
+        self.graph_blocks = 0
         while it < maxiter:
-            if it % check_every == 0:
-                if rel_tol is None:
-                    active = active & (res >= tol)
-                else:
-                    rn = torch.sqrt(torch.clamp(self.dot(r, r), min=0.0)) / bnorm
-                    if history is not None:
-                        history.append(rn.cpu().numpy())
-                    active = active & ~(rn < rel_tol)
-                if not bool(active.any()):
-                    break
-                engine.check_timeouts("Wiener filter")
-            Ap = self.apply_A(p)
-            pAp = self.dot(p, Ap)
-            alpha = torch.where(active, res / torch.where(pAp != 0, pAp, torch.ones_like(pAp)), torch.zeros_like(res))
-            x = x + bc(alpha) * p
-            iters = iters + active.to(torch.int64)
-            it += 1
-            if refine_every and it % refine_every == 0:
-                r = torch.where(bc(active), b - self.apply_A(x, "f64"), r)
+            if history is not None and S["rel_tol"] is not None:
+                history.append(S["rn"].cpu().numpy())
+            if not bool(S["active"].any()):  # one host synchronisation per block
+                break
+            engine.check_timeouts("Wiener filter")
+            m = min(k, maxiter - it)
+            refine_at = [j for j in range(m) if refine_every and (it + j + 1) % refine_every == 0]
+            full = m == k and it % k == 0
+            if use_graphs and full and it > 0:
+                if graph is None:  # no device-wide synchronisation: other threads may be capturing too
+                    def block():
+                        for j in range(m):
+                            self._iteration(S, j in refine_at)
+                    graph = engine.capture_graph(block)
+                graph.replay()
+                self.graph_blocks += 1
             else:
-                r = r - bc(alpha) * Ap
-            z = self._apply(self.P_inv, r)
-            res_new = self.dot(r, z)
-            beta = torch.where(active, res_new / torch.where(res != 0, res, torch.ones_like(res)), torch.zeros_like(res))
-            p = z + bc(beta) * p
-            res = torch.where(active, res_new, res)
-        its = iters.cpu().tolist()
+                for j in range(m):
+                    self._iteration(S, j in refine_at)
+            it += m
+        its = S["iters"].cpu().tolist()
         engine.check_timeouts("Wiener filter")
+        x = S["x"]
         if self.batch == 1:
             return x[0], its[0]
         return x, its

@@ -123,6 +123,18 @@ int lf_lense_flow_vjp(lf_plan_t plan, const void* f_lensed, const void* cotangen
                       int batch, int nsteps, int direction, void* delta_f, void* f_back, void* dphi, int dphi_basis,
                       void* workspace, size_t workspace_bytes, void* stream);
 
+/* Per-mode products of Fourier-diagonal C x C operators with fields, as the
+ * Wiener filter's operator applies them (the products of
+ * matrix_operators.py:54-141 and the EB<->QU rotations of util.py:140-161,
+ * composed per mode):  out[b][i][m] = scale * sum_j W[b][i][j][m] X[b][j][m]
+ * + yscale * Y[b][i][m].  W: real float64 [batch or 1][ncomp][ncomp][modes]
+ * (w_batched = 0 broadcasts one operator); X, Y, out: complex128
+ * [batch][ncomp][modes] (interleaved re, im); Y may be NULL.  Bit i*ncomp+j
+ * of ``nonzero`` marks the blocks of W that are not identically zero (the
+ * others are skipped).  out may alias X or Y. */
+int lf_modes_apply(const void* W, int w_batched, unsigned nonzero, const void* X, const void* Y, void* out, int batch,
+                   int ncomp, long modes, double scale, double yscale, void* stream);
+
 /* Checkpointed exact reverse pass: the transpose of the discrete forward map
  * f -> L(phi) f that lf_lense_flow computes (direction +1 or -1, standard
  * RHS), for the cotangent ``cotangent`` and the UNLENSED field ``f_in`` -- the

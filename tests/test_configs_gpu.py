@@ -308,3 +308,63 @@ def test_grad_phi_exact_scheme_256_IQU(torch_cuda):
     go = R.grad_phi_logpdf(So["field"], So["phi"], So["data"], So["Cn"], So["Cphi"], So["Cf"], So["M"], So["B"], n=7,
                            scheme="exact")
     assert rel_l2(g32.scalar_matrix, go) < 2e-5
+
+
+@pytest.mark.parametrize("C,batched", [(1, False), (2, True), (3, True), (3, False)])
+def test_modes_apply_matches_torch(torch_cuda, C, batched):
+    """lf_modes_apply (the Wiener filter's fused per-mode operator product) against torch, zero blocks skipped,
+    in place and with the Y term."""
+    import ctypes
+    torch = torch_cuda
+    from cmblensing_b200 import _native as nat
+    from cmblensing_b200.wf_engine import _nonzero_mask
+    lib = nat.load()
+    B, N = 3, 64
+    H = N // 2 + 1
+    g = torch.Generator(device="cpu").manual_seed(C)
+    W = torch.randn(((B,) if batched else ()) + (C, C, N, H), generator=g, dtype=torch.float64)
+    if C == 3:
+        W[..., 0, 2, :, :] = 0
+        W[..., 2, 0, :, :] = 0
+    W = W.cuda()
+    X = torch.randn((B, C, N, H), generator=g, dtype=torch.complex128).cuda()
+    Y = torch.randn((B, C, N, H), generator=g, dtype=torch.complex128).cuda()
+    Wb = W if batched else W.unsqueeze(0).expand(B, *W.shape)
+    ref = 0.5 * torch.einsum("bijnh,bjnh->binh", Wb.to(torch.complex128), X) - 2.0 * Y
+    nz = _nonzero_mask(W)
+    if C == 3:
+        assert not nz & (1 << 2) and not nz & (1 << 6)
+    vp = lambda t: ctypes.c_void_p(t.data_ptr())
+    st = ctypes.c_void_p(torch.cuda.current_stream().cuda_stream)
+    out = torch.empty_like(X)
+    assert lib.lf_modes_apply(vp(W), int(batched), nz, vp(X), vp(Y), vp(out), B, C, N * H, 0.5, -2.0, st) == 0
+    Xi = X.clone()  # in place: out aliases X
+    assert lib.lf_modes_apply(vp(W), int(batched), nz, vp(Xi), vp(Y), vp(Xi), B, C, N * H, 0.5, -2.0, st) == 0
+    torch.cuda.synchronize()
+    assert rel_l2(out.cpu().numpy(), ref.cpu().numpy()) < 1e-14
+    assert torch.equal(out, Xi)
+
+
+def test_wiener_filter_graph_replay_equals_eager(torch_cuda):
+    """The CG blocks replayed from a captured CUDA graph give the eager iterations' iterates and counts."""
+    import cmblensing_b200 as cl
+    from cmblensing_b200 import matrix_operators as mo
+    from cmblensing_b200.simulate import hole_mask
+    from cmblensing_b200.wf_engine import DeviceWienerFilter
+
+    class Mod:
+        FlatS0, FlatS2, FlatS02 = cl.FlatS0, cl.FlatS2, cl.FlatS02
+        DiagonalScalar, DiagonalEB, BlockTEB = mo.DiagonalScalar, mo.DiagonalEB, mo.BlockTEB
+
+    probs = []
+    for seed in (21, 22):
+        S = _problem(Mod, 128, 2.0, "P", 1.0, 2.0, 2.0, seed=seed, bb_fraction=0.01,
+                     mask=hole_mask(128, 2.0, nholes=5, seed=seed))
+        probs.append(dict(phi=S["phi"], data=S["data"], Cf=S["Cf"], Cn=S["Cn"], M=S["M"], B=S["B"]))
+    wf = DeviceWienerFilter(problems=probs, n=7)
+    xg, itg = wf.solve(rel_tol=1e-8, refine_every=10, use_graphs=True)
+    assert wf.graph_blocks >= 1
+    xe, ite = wf.solve(rel_tol=1e-8, refine_every=10, use_graphs=False)
+    assert wf.graph_blocks == 0
+    assert itg == ite
+    assert torch_cuda.equal(xg, xe)

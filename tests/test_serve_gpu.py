@@ -54,12 +54,14 @@ def test_mixed_stream_equals_solo_runs(torch_cuda):
     from cmblensing_b200.serve import Server, latency_summary, run_alone
     reqs = []
     rng = np.random.default_rng(0)
-    for i in range(24):
-        N = [64, 128, 256][rng.integers(3)]
+    for i in range(32):  # the workload's grid sizes
+        N = [128, 256, 512, 1024][rng.integers(4)]
         C = [1, 2][rng.integers(2)]
         kind = ["lens", "delens"][rng.integers(2)]
-        reqs.append(_lens_req(kind, N, C, 3.0 if N < 256 else 2.0, seed=10 * i))
-    reqs += [_wf_req(64, seed=s) for s in (1, 2, 3)]
+        reqs.append(_lens_req(kind, N, C, 3.0 if N < 512 else 2.0, seed=10 * i))
+    # Wiener filters of three sizes: two workers solve (and capture their CG graphs) concurrently
+    reqs += [_wf_req(64, seed=s) for s in (1, 2, 3)] + [_wf_req(128, seed=4), _wf_req(512, seed=5)]
+    rng.shuffle(reqs)
     srv = Server(max_batch=8, wf_workers=2).start()
     for r in reqs:
         srv.submit(r)
