@@ -47,6 +47,9 @@ SIGNATURES = {
     "lf_min_det_init": (_i, [_vp, _i, _vp]),
     "lf_decode_min_det": (ctypes.c_float, [_i]),
     "lf_lense_flow": (_i, [_vp, _vp, _i, _vp, _i, _vp, _i, _i, _i, _i, _vp, _sz, _vp]),
+    "lf_pp_bytes": (_sz, [_vp, _i, _i]),
+    "lf_phi_precompute_pp": (_i, [_vp, _vp, _i, _i, _vp, _vp, _i, _vp, _vp, _sz, _vp]),
+    "lf_lense_flow_pp": (_i, [_vp, _vp, _i, _vp, _i, _vp, _i, _i, _i, _i, _vp, _sz, _vp]),
     "lf_fft_workspace_bytes": (_sz, [_vp, _i]),
     "lf_rfft2": (_i, [_vp, _vp, _i, _i, _vp, _vp]),
     "lf_irfft2": (_i, [_vp, _vp, _i, _vp, _i, _vp, _sz, _vp]),

@@ -244,8 +244,12 @@ cudaError_t launch_col(int planes, cudaStream_t st, const StageArgs& a) {
   }
 }
 
+// The p planes hold p = M(t)^-1 grad(phi) at the 2n+1 times k / (2n), k = 0..2n, ascending; an
+// integration from t0 = 1 reads time t0 + k hh at index 2n - k.  ``pp_given``: the caller supplies
+// them (lf_lense_flow_pp), otherwise k_p_planes forms them from the derivative planes first.
 template <typename T, int N, int C, bool ADJ, bool PP>
-cudaError_t run_lens_pp(const StageArgs& base, int B, int nsteps, double t0, double t1, cudaStream_t st) {
+cudaError_t run_lens_pp(const StageArgs& base, int B, int nsteps, double t0, double t1, cudaStream_t st,
+                        bool pp_given = false) {
   constexpr int RL = Geo<T>::ROW_LINES;
   constexpr int RNT = Geo<T>::row_nt(N);
   constexpr int RMB = Geo<T>::row_minb(N, C);
@@ -257,20 +261,24 @@ cudaError_t run_lens_pp(const StageArgs& base, int B, int nsteps, double t0, dou
   const double h = (t1 - t0) / nsteps;  // util.py:185
   const double hh = h / 2.0;
   if constexpr (PP) {
-    // p at the stage times t0 + k hh, k = 0..2n
-    const long P = (long)N * N;
     a.pp_k = 2 * nsteps + 1;
-    const int gx = (int)std::min<long>((P / 2 + 255) / 256, 1024);
-    e = launch_k<k_p_planes<T>>(LF_KIND_PP, dim3(gx, B), 256, 0, st, reinterpret_cast<const T*>(a.phi),
-                                reinterpret_cast<T*>(const_cast<void*>(a.pp)), P, a.pp_k, t0, hh);
-    if (e != cudaSuccess) return e;
+    if (!pp_given) {  // p at the times k / (2n), ascending
+      const long P = (long)N * N;
+      const int gx = (int)std::min<long>((P / 2 + 255) / 256, 1024);
+      e = launch_k<k_p_planes<T>>(LF_KIND_PP, dim3(gx, B), 256, 0, st, reinterpret_cast<const T*>(a.phi),
+                                  reinterpret_cast<T*>(const_cast<void*>(a.pp)), P, a.pp_k, 0.0,
+                                  0.5 / nsteps);
+      if (e != cudaSuccess) return e;
+    }
   }
+  const bool rev = t0 != 0.0;  // time t0 + k hh sits at index 2n - k
+  auto pidx = [=](int k) { return rev ? 2 * nsteps - k : k; };
   a.h = h;
   a.stage = 0;
   a.last = 0;
   a.t_cur = t0;
   a.t_next = t0;
-  a.pp_idx = 0;
+  a.pp_idx = pidx(0);
   // Programmatic dependent launch for small batches (up to 2^23 pixels, 16 maps of 512^2 QU):
   // measured per 512^2 QU lens with the phi precompute, 4 maps 0.79 -> 0.66 ms, 16 maps 2.35 ->
   // 2.25 ms, but 64 maps 7.85 -> 8.13 ms.  The initial transform follows k_p_planes (which has no
@@ -293,7 +301,7 @@ cudaError_t run_lens_pp(const StageArgs& base, int B, int nsteps, double t0, dou
       a.stage = s + 1;
       a.t_cur = tc[s];
       a.t_next = tn[s];
-      a.pp_idx = ADJ ? kn[s] : kc[s];
+      a.pp_idx = pidx(ADJ ? kn[s] : kc[s]);
       a.last = (i == nsteps - 1 && s == 3);
       e = launch_col<T, N>(B * C, st, a);
       if (e != cudaSuccess) return e;
@@ -320,30 +328,30 @@ cudaError_t run_lens_pp(const StageArgs& base, int B, int nsteps, double t0, dou
 
 // The p-plane path (a.pp set) is built for float32 plans only.
 template <typename T, int N, int C, bool ADJ>
-cudaError_t run_lens_n(const StageArgs& a, int B, int nsteps, double t0, double t1, cudaStream_t st) {
+cudaError_t run_lens_n(const StageArgs& a, int B, int nsteps, double t0, double t1, cudaStream_t st, bool pp_given) {
   if constexpr (std::is_same<T, float>::value) {
-    if (a.pp) return run_lens_pp<T, N, C, ADJ, true>(a, B, nsteps, t0, t1, st);
+    if (a.pp) return run_lens_pp<T, N, C, ADJ, true>(a, B, nsteps, t0, t1, st, pp_given);
   }
   return run_lens_pp<T, N, C, ADJ, false>(a, B, nsteps, t0, t1, st);
 }
 
 template <typename T, int N>
 cudaError_t run_lens_c(int C, bool adj, const StageArgs& a, int B, int nsteps, double t0, double t1,
-                       cudaStream_t st) {
-  if (C == 1) return adj ? run_lens_n<T, N, 1, true>(a, B, nsteps, t0, t1, st) : run_lens_n<T, N, 1, false>(a, B, nsteps, t0, t1, st);
-  if (C == 2) return adj ? run_lens_n<T, N, 2, true>(a, B, nsteps, t0, t1, st) : run_lens_n<T, N, 2, false>(a, B, nsteps, t0, t1, st);
-  return adj ? run_lens_n<T, N, 3, true>(a, B, nsteps, t0, t1, st) : run_lens_n<T, N, 3, false>(a, B, nsteps, t0, t1, st);
+                       cudaStream_t st, bool pp_given) {
+  if (C == 1) return adj ? run_lens_n<T, N, 1, true>(a, B, nsteps, t0, t1, st, pp_given) : run_lens_n<T, N, 1, false>(a, B, nsteps, t0, t1, st, pp_given);
+  if (C == 2) return adj ? run_lens_n<T, N, 2, true>(a, B, nsteps, t0, t1, st, pp_given) : run_lens_n<T, N, 2, false>(a, B, nsteps, t0, t1, st, pp_given);
+  return adj ? run_lens_n<T, N, 3, true>(a, B, nsteps, t0, t1, st, pp_given) : run_lens_n<T, N, 3, false>(a, B, nsteps, t0, t1, st, pp_given);
 }
 
 template <typename T>
 cudaError_t run_lens(int N, int C, bool adj, const StageArgs& a, int B, int nsteps, double t0, double t1,
-                     cudaStream_t st) {
+                     cudaStream_t st, bool pp_given = false) {
   switch (N) {
-    case 64: return run_lens_c<T, 64>(C, adj, a, B, nsteps, t0, t1, st);
-    case 128: return run_lens_c<T, 128>(C, adj, a, B, nsteps, t0, t1, st);
-    case 256: return run_lens_c<T, 256>(C, adj, a, B, nsteps, t0, t1, st);
-    case 512: return run_lens_c<T, 512>(C, adj, a, B, nsteps, t0, t1, st);
-    default: return run_lens_c<T, 1024>(C, adj, a, B, nsteps, t0, t1, st);
+    case 64: return run_lens_c<T, 64>(C, adj, a, B, nsteps, t0, t1, st, pp_given);
+    case 128: return run_lens_c<T, 128>(C, adj, a, B, nsteps, t0, t1, st, pp_given);
+    case 256: return run_lens_c<T, 256>(C, adj, a, B, nsteps, t0, t1, st, pp_given);
+    case 512: return run_lens_c<T, 512>(C, adj, a, B, nsteps, t0, t1, st, pp_given);
+    default: return run_lens_c<T, 1024>(C, adj, a, B, nsteps, t0, t1, st, pp_given);
   }
 }
 
@@ -380,6 +388,51 @@ cudaError_t run_phi_n(const void* phi, int basis, int B, TO* planes, int* min_de
     e = launch<k_min_det<TO>>(dim3(32, B), 256, 0, st, (const TO*)planes, P, min_det);
   }
   return e;
+}
+
+// The phi precompute with the p planes formed in the derivative row pass (float32 plans):
+// rfft2 of phi (or its given spectrum), the three inverse column transforms of the five
+// derivatives, then k_phi_rows_c2r_pp over 4-row tiles of all five.
+template <int N>
+cudaError_t run_phi_pp_n(const void* phi, int basis, int B, float* planes, float* pp, int K, int* min_det, void* ws,
+                         const double2* tw64, double kbase, cudaStream_t st) {
+  constexpr int LINES = 8, PL = 4;
+  constexpr int NT = Geo<double>::nt(N);
+  constexpr int H = N / 2;
+  double2* spec = reinterpret_cast<double2*>(ws);
+  double2* packed = spec + (size_t)B * N * (H + 1);
+  const size_t smem_row = sizeof(double2) * (N + LINES * H) + 16;
+  const size_t smem_col = sizeof(double2) * (N + LINES * N) + 16;
+  const size_t smem_pp = sizeof(double2) * (N + 5 * PL * H) + 16;
+  const int ctiles = (H + 1 + LINES - 1) / LINES;
+  cudaError_t e;
+  if (basis == LF_PHI_MAP) {
+    e = launch<k_phi_rows_r2c<N, LINES, NT>>(dim3(N / LINES, B), NT, smem_row, st,
+                                             reinterpret_cast<const double*>(phi), spec, tw64);
+    if (e != cudaSuccess) return e;
+    e = launch<k_phi_cols_fwd<N, LINES, NT>>(dim3(ctiles, B), NT, smem_col, st, spec, tw64);
+    if (e != cudaSuccess) return e;
+  } else {
+    e = cudaMemcpyAsync(spec, phi, sizeof(double2) * (size_t)B * N * (H + 1), cudaMemcpyDeviceToDevice, st);
+    if (e != cudaSuccess) return e;
+  }
+  e = launch<k_phi_cols_deriv<N, LINES, NT>>(dim3(ctiles, B), NT, smem_col, st, (const double2*)spec, packed,
+                                             (const double2*)tw64, kbase);
+  if (e != cudaSuccess) return e;
+  constexpr int NTP = pp_threads(N);
+  return launch<k_phi_rows_c2r_pp<N, PL, NTP>>(dim3(N / PL, B), NTP, smem_pp, st, (const double2*)packed, planes, pp,
+                                               K, min_det, (const double2*)tw64);
+}
+
+cudaError_t run_phi_pp(int N, const void* phi, int basis, int B, float* planes, float* pp, int K, int* min_det,
+                       void* ws, const double2* tw64, double kbase, cudaStream_t st) {
+  switch (N) {
+    case 64: return run_phi_pp_n<64>(phi, basis, B, planes, pp, K, min_det, ws, tw64, kbase, st);
+    case 128: return run_phi_pp_n<128>(phi, basis, B, planes, pp, K, min_det, ws, tw64, kbase, st);
+    case 256: return run_phi_pp_n<256>(phi, basis, B, planes, pp, K, min_det, ws, tw64, kbase, st);
+    case 512: return run_phi_pp_n<512>(phi, basis, B, planes, pp, K, min_det, ws, tw64, kbase, st);
+    default: return run_phi_pp_n<1024>(phi, basis, B, planes, pp, K, min_det, ws, tw64, kbase, st);
+  }
 }
 
 template <typename TO>
@@ -921,6 +974,69 @@ int lf_lense_flow(lf_plan_t p, const void* f_in, int in_dtype, void* f_out, int 
   else
     e = run_lens<float>(p->N, p->C, adj, a, batch, nsteps, t0, t1, st);
   return cuda_status(e);
+}
+
+size_t lf_pp_bytes(lf_plan_t p, int batch, int nsteps) {
+  if (!p || batch < 0 || nsteps < 1) return 0;
+  return pp_bytes(p, batch, nsteps);
+}
+
+int lf_phi_precompute_pp(lf_plan_t p, const void* phi, int basis, int batch, void* planes, void* pp, int nsteps,
+                         int* min_det, void* ws, size_t ws_bytes, void* stream) {
+  if (!p) return LF_ERR_BAD_ARG;
+  if (timeout_recorded()) return LF_ERR_TIMEOUT;
+  if (p->prec != LF_F32) return LF_ERR_BAD_DTYPE;
+  if (batch < 0) return LF_ERR_BAD_SHAPE;
+  if (basis != LF_PHI_MAP && basis != LF_PHI_FOURIER) return LF_ERR_BAD_ARG;
+  if (nsteps < 1) return LF_ERR_BAD_ARG;
+  if (batch == 0) return LF_OK;
+  if (!phi || !pp || !ws || !aligned16(phi) || !aligned16(pp) || !aligned16(ws) || (planes && !aligned16(planes)))
+    return LF_ERR_BAD_ARG;
+  if (ws_bytes < lf_phi_workspace_bytes(p, batch)) return LF_ERR_WORKSPACE;
+  const double kbase = 2.0 * M_PI / ((double)p->N * p->pix_width);
+  g_prof = &p->prof;
+  return cuda_status(run_phi_pp(p->N, phi, basis, batch, reinterpret_cast<float*>(planes), reinterpret_cast<float*>(pp),
+                                2 * nsteps + 1, min_det, ws, p->tw64, kbase, (cudaStream_t)stream));
+}
+
+int lf_lense_flow_pp(lf_plan_t p, const void* f_in, int in_dtype, void* f_out, int out_dtype, const void* pp,
+                     int batch, int nsteps, int direction, int adjoint, void* ws, size_t ws_bytes, void* stream) {
+  if (!p) return LF_ERR_BAD_ARG;
+  if (timeout_recorded()) return LF_ERR_TIMEOUT;
+  if (p->prec != LF_F32) return LF_ERR_BAD_DTYPE;
+  if (batch < 0) return LF_ERR_BAD_SHAPE;
+  if ((in_dtype != LF_F32 && in_dtype != LF_F64) || (out_dtype != LF_F32 && out_dtype != LF_F64))
+    return LF_ERR_BAD_DTYPE;
+  if (nsteps < 1 || (direction != LF_FORWARD_LENSE && direction != LF_INVERSE_LENSE)) return LF_ERR_BAD_ARG;
+  if (batch == 0) return LF_OK;
+  if (!f_in || !f_out || !pp || !ws || !aligned16(f_in) || !aligned16(f_out) || !aligned16(pp) || !aligned16(ws))
+    return LF_ERR_BAD_ARG;
+  const bool adj = adjoint != 0;
+  if (ws_bytes < lf_workspace_bytes(p, batch, adj)) return LF_ERR_WORKSPACE;
+  const bool fwd_time = ((direction == LF_FORWARD_LENSE) != adj);
+  const double t0 = fwd_time ? 0.0 : 1.0, t1 = fwd_time ? 1.0 : 0.0;
+  const size_t plane_bytes = 4 * (size_t)p->N * p->N * (size_t)batch * p->C;
+  StageArgs a;
+  std::memset(&a, 0, sizeof(a));
+  a.f_in = f_in;
+  a.f_out = f_out;
+  a.in_f64 = in_dtype == LF_F64;
+  a.out_f64 = out_dtype == LF_F64;
+  a.phi = pp;  // not read on the p-plane path
+  a.pp = pp;
+  char* w = reinterpret_cast<char*>(ws);
+  a.y0 = w;
+  a.acc = w + plane_bytes;
+  a.s = w + 2 * plane_bytes;
+  a.gx = w + 3 * plane_bytes;
+  a.v = adj ? (void*)(w + 4 * plane_bytes) : nullptr;
+  a.twN = p->tw;
+  a.twP = p->twp;
+  a.twC = p->twc();
+  a.kbase = 2.0 * M_PI / ((double)p->N * p->pix_width);
+  a.nplanes = batch * p->C;
+  g_prof = &p->prof;
+  return cuda_status(run_lens<float>(p->N, p->C, adj, a, batch, nsteps, t0, t1, (cudaStream_t)stream, true));
 }
 
 int lf_wait_timeouts(int* count, int reset) {

@@ -1091,6 +1091,99 @@ __global__ void k_min_det(const T* __restrict__ planes, long P, int* __restrict_
   if ((threadIdx.x & 31) == 0) atomicMin(out + map, ordered_int(float(best)));
 }
 
+// ============================ fused: derivative rows -> p planes at the stage times
+// The inverse real row transforms of all five derivative spectra of LINES
+// rows (as k_phi_rows_c2r, float64), and in the same block, from the five
+// derivatives of each pixel held in float64: p = M(t)^-1 grad(phi)
+// (lense_flow.py:373-381, :398-415) at the K = 2n+1 times k / (2n), stored
+// float32 ascending in time ([B][K][2][N][N]), and the per-map minimum of
+// det(I + t grad grad phi) over pixels and t in [0, 1] (as k_min_det).  The
+// five derivative planes are written only when ``planes`` is non-null, so
+// the forward lens's p planes no longer round-trip them through HBM.
+// grid: x = row tile, y = map.  NT: one first-pass butterfly per thread (a warp multiple).
+__host__ __device__ constexpr int pp_threads(int n) { return n <= 64 ? 96 : (n == 128 ? 160 : (n <= 512 ? 320 : 512)); }
+
+template <int N, int LINES, int NT>
+__global__ void __launch_bounds__(NT, N == 1024 ? 1 : 2) k_phi_rows_c2r_pp(const double2* __restrict__ packed, float* __restrict__ planes,
+                                                         float* __restrict__ pp, int K, int* __restrict__ min_det,
+                                                         const double2* __restrict__ twN) {
+  constexpr int H = N / 2;
+  constexpr long P = (long)N * N;
+  constexpr int TILE = LINES * H;
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  double2* tw = reinterpret_cast<double2*>(smem_raw);
+  double2* buf = tw + N;  // derivative j at buf + j * TILE
+  __shared__ double warp_min[NT / 32];
+  const int tid = threadIdx.x;
+  const int r0 = blockIdx.x * LINES;
+  const long map = blockIdx.y;
+  uint64_t* mbar = reinterpret_cast<uint64_t*>(buf + 5 * TILE);
+  table_copy<N>(tw, twN, mbar, tid);
+#pragma unroll
+  for (int j = 0; j < 5; ++j)
+    load_rows<double, double2, H, LINES, NT>(buf + j * TILE, packed + ((map * 5 + j) * N + r0) * (long)H, H, tid);
+  __syncthreads();
+  table_wait(mbar);
+  c2r_pre<double, H, LINES, 5, NT>(buf, tw, tid);
+  fft_tiles<double, H, LINES, 5, NT, true, N>(buf, tw, tid);
+  // tile element m of a row holds pixels 2m (re) and 2m + 1 (im); two elements (four pixels) per item
+  const double inv2n = 1.0 / double(K - 1);
+  double best = 1.0;
+  for (int idx = tid; idx < LINES * (H / 2); idx += NT) {
+    const int row = idx / (H / 2), m0 = 2 * (idx % (H / 2));
+    double d[5][4];
+#pragma unroll
+    for (int j = 0; j < 5; ++j) {
+      const double2 a0 = buf[j * TILE + sw<double, LINES>(m0, row)];
+      const double2 a1 = buf[j * TILE + sw<double, LINES>(m0 + 1, row)];
+      d[j][0] = a0.x;
+      d[j][1] = a0.y;
+      d[j][2] = a1.x;
+      d[j][3] = a1.y;
+    }
+    const long o = (long)(r0 + row) * N + 2 * m0;  // first of the four pixels
+    if (planes) {
+#pragma unroll
+      for (int j = 0; j < 5; ++j)
+        *reinterpret_cast<float4*>(planes + (map * 5 + j) * P + o) =
+            make_float4(float(d[j][0]), float(d[j][1]), float(d[j][2]), float(d[j][3]));
+    }
+#pragma unroll
+    for (int q = 0; q < 4; ++q) {  // min over t in [0, 1] of det(I + t H) = 1 + t l + t^2 qd
+      const double A = d[2][q], B = d[3][q], Cc = d[4][q];
+      const double qd = A * Cc - B * B, l = A + Cc;
+      double dm = 1.0 + l + qd;
+      if (qd > 0.0) {
+        const double ts = -l / (2.0 * qd);
+        if (ts > 0.0 && ts < 1.0) dm = fmin(dm, 1.0 + ts * l + ts * ts * qd);
+      }
+      best = fmin(best, dm);
+    }
+    float* out = pp + map * (long)K * 2 * P + o;
+#pragma unroll 1
+    for (int k = 0; k < K; ++k) {
+      const double t = double(k) * inv2n;
+      double ox[4], oy[4];
+#pragma unroll
+      for (int q = 0; q < 4; ++q) p_vector<double>(d[0][q], d[1][q], d[2][q], d[3][q], d[4][q], t, ox[q], oy[q]);
+      *reinterpret_cast<float4*>(out + (2 * k) * P) =
+          make_float4(float(ox[0]), float(ox[1]), float(ox[2]), float(ox[3]));
+      *reinterpret_cast<float4*>(out + (2 * k + 1) * P) =
+          make_float4(float(oy[0]), float(oy[1]), float(oy[2]), float(oy[3]));
+    }
+  }
+  if (min_det) {
+    for (int w = 16; w > 0; w >>= 1) best = fmin(best, __shfl_xor_sync(0xffffffffu, best, w));
+    if ((tid & 31) == 0) warp_min[tid / 32] = best;
+    __syncthreads();
+    if (tid == 0) {
+      double b = warp_min[0];
+      for (int w = 1; w < NT / 32; ++w) b = fmin(b, warp_min[w]);
+      atomicMin(min_det + map, ordered_int(float(b)));
+    }
+  }
+}
+
 // ======================================================= reverse mode
 // delta-phi accumulation for one RK4 stage (lense_flow.py:195-252).  With
 // fdf = sum_c df_c grad f_c, a = M^-1 fdf, w = p (x) a, the stage rate is

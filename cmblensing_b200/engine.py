@@ -108,6 +108,83 @@ class Plan:
                                                      f"min det(I + t grad grad phi) = {min(vals):.3g}")
         return planes
 
+    def pp_bytes(self, batch, n):
+        """Bytes of the stage-time p planes of ``batch`` maps for ``n`` RK4 steps (float32 plans)."""
+        return int(self._lib.lf_pp_bytes(self.handle, int(batch), int(n)))
+
+    def phi_pp(self, phi, n, check_det=True, out=None, planes_out=None, workspace=None, min_det=None):
+        """p = M(t)^-1 grad(phi) at the 2n+1 times k/(2n) for [B,N,N] map / [B,N,N/2+1] Fourier phi
+        (lf_phi_precompute_pp; float32 plans): a [B, 2n+1, 2, N, N] float32 tensor, formed in float64 in the
+        derivative row pass.  ``planes_out`` optionally receives the five derivative planes.  With
+        ``check_det`` the magnification minimum is read back as in ``phi_planes``; a caller-owned int32
+        ``min_det`` buffer (initialised with lf_min_det_init) is filled without a readback instead."""
+        if self.prec_code != nat.LF_F32:
+            raise nat.LenseFlowError(nat.LF_ERR_BAD_DTYPE, "p planes need a float32 plan")
+        N = self.nside
+        if phi.dim() == 2:
+            phi = phi.unsqueeze(0)
+        if phi.shape[-2:] == (N, N):
+            basis = nat.LF_PHI_MAP
+            phi = phi.to(device=self.device, dtype=torch.float64).contiguous()
+        elif phi.shape[-2:] == (N, N // 2 + 1):
+            basis = nat.LF_PHI_FOURIER
+            phi = phi.to(device=self.device, dtype=torch.complex128).contiguous()
+        else:
+            raise nat.LenseFlowError(nat.LF_ERR_BAD_SHAPE, f"phi shape {tuple(phi.shape)} for N={N}")
+        B, K = phi.shape[0], 2 * int(n) + 1
+        pp = out if out is not None else torch.empty((B, K, 2, N, N), dtype=torch.float32, device=self.device)
+        if pp.shape != (B, K, 2, N, N) or pp.dtype != torch.float32 or not pp.is_contiguous():
+            raise nat.LenseFlowError(nat.LF_ERR_BAD_SHAPE, "p-plane buffer does not match")
+        if planes_out is not None and (planes_out.shape != (B, 5, N, N) or planes_out.dtype != torch.float32):
+            raise nat.LenseFlowError(nat.LF_ERR_BAD_SHAPE, "derivative plane buffer does not match")
+        ws = workspace
+        if ws is None or ws.numel() < self.phi_workspace_bytes(B):
+            ws = torch.empty(max(self.phi_workspace_bytes(B), 16), dtype=torch.uint8, device=self.device)
+        md = min_det
+        if md is None and check_det:
+            md = torch.empty(max(B, 1), dtype=torch.int32, device=self.device)
+        with torch.cuda.device(self.device):
+            st = _stream_ptr(self.device)
+            if md is not None and min_det is None:
+                nat.check(self._lib.lf_min_det_init(_ptr(md), B, st), "lf_min_det_init")
+            nat.check(self._lib.lf_phi_precompute_pp(self.handle, _ptr(phi), basis, B,
+                                                     _ptr(planes_out) if planes_out is not None else None, _ptr(pp),
+                                                     int(n), _ptr(md) if md is not None else None, _ptr(ws),
+                                                     ws.numel(), st), "lf_phi_precompute_pp")
+        if md is not None and min_det is None:
+            vals = [self._lib.lf_decode_min_det(int(v)) for v in md.cpu().tolist()[:B]]
+            check_timeouts("lf_phi_precompute_pp")
+            self.last_min_det = vals
+            if not all(v > 0.0 for v in vals):
+                raise nat.SingularMagnificationError(nat.LF_ERR_SINGULAR_MAGNIFICATION,
+                                                     f"min det(I + t grad grad phi) = {min(vals):.3g}")
+        return pp
+
+    def lense_flow_pp(self, f, pp, n, direction=FORWARD_LENSE, adjoint=False, out=None, workspace=None,
+                      out_dtype=None):
+        """LenseFlow with precomputed p planes (from ``phi_pp`` with the same n): lf_lense_flow_pp."""
+        N, C = self.nside, self.ncomp
+        if f.dim() != 4 or f.shape[1:] != (C, N, N):
+            raise nat.LenseFlowError(nat.LF_ERR_BAD_SHAPE, f"field shape {tuple(f.shape)} for C={C}, N={N}")
+        if f.dtype not in (torch.float32, torch.float64):
+            raise nat.LenseFlowError(nat.LF_ERR_BAD_DTYPE, str(f.dtype))
+        f = f.contiguous()
+        B = f.shape[0]
+        if pp.shape != (B, 2 * int(n) + 1, 2, N, N) or pp.dtype != torch.float32 or not pp.is_contiguous():
+            raise nat.LenseFlowError(nat.LF_ERR_BAD_SHAPE, "p planes do not match the field batch / n")
+        odt = f.dtype if out_dtype is None else out_dtype
+        if out is None:
+            out = torch.empty((B, C, N, N), dtype=odt, device=self.device)
+        if workspace is None or workspace.numel() < self.workspace_bytes(B, adjoint):
+            workspace = torch.empty(max(self.workspace_bytes(B, adjoint), 16), dtype=torch.uint8, device=self.device)
+        code = lambda t: nat.LF_F64 if t == torch.float64 else nat.LF_F32
+        with torch.cuda.device(self.device):
+            nat.check(self._lib.lf_lense_flow_pp(self.handle, _ptr(f), code(f.dtype), _ptr(out), code(out.dtype),
+                                                 _ptr(pp), B, int(n), int(direction), int(bool(adjoint)),
+                                                 _ptr(workspace), workspace.numel(), _stream_ptr(self.device)),
+                      "lf_lense_flow_pp")
+        return out
+
     # ------------------------------------------------------------ lens
     def lense_flow(self, f, planes, n=10, direction=FORWARD_LENSE, adjoint=False, out=None, workspace=None,
                    out_dtype=None):
@@ -321,8 +398,14 @@ class HostPipeline:
         self.d_f = [torch.empty((cb, C, N, N), dtype=io_dtype, device=dev) for _ in range(ns)]
         self.d_out = [torch.empty((cb, C, N, N), dtype=io_dtype, device=dev) for _ in range(ns)]
         self.d_phi = [torch.empty((cb, N, N), dtype=torch.float64, device=dev) for _ in range(ns)]
-        self.planes = [torch.empty((cb, 5, N, N), dtype=plan.dtype, device=dev) for _ in range(ns)]
-        self.ws = [torch.empty(16, dtype=torch.uint8, device=dev) for _ in range(ns)]  # sized for n at first call
+        # float32 plans: the phi precompute writes the stage-time p planes directly (lf_phi_precompute_pp), one
+        # set per slot and step count, kept while graphs that use them may replay; float64: derivative planes
+        self.use_pp = plan.prec_code == nat.LF_F32
+        self.pp = {}  # n -> per-slot p-plane buffers
+        self.planes = [] if self.use_pp else [torch.empty((cb, 5, N, N), dtype=plan.dtype, device=dev)
+                                              for _ in range(ns)]
+        self.ws = [torch.empty(max(plan.workspace_bytes(cb, True), 16), dtype=torch.uint8, device=dev)
+                   for _ in range(ns)]
         self.phi_ws = [torch.empty(max(plan.phi_workspace_bytes(cb), 16), dtype=torch.uint8, device=dev)
                        for _ in range(ns)]
         # magnification minima of the two most recent calls
@@ -344,10 +427,19 @@ class HostPipeline:
         plan, lib = self.plan, self.plan._lib
         st = _stream_ptr(plan.device)
         md = _ptr(self.min_det[ring][lo:]) if check_det else None
+        code = nat.LF_F64 if self.io_dtype == torch.float64 else nat.LF_F32
+        if self.use_pp:
+            pp = self.pp[n][slot]
+            nat.check(lib.lf_phi_precompute_pp(plan.handle, _ptr(self.d_phi[slot]), nat.LF_PHI_MAP, m, None, _ptr(pp),
+                                               int(n), md, _ptr(self.phi_ws[slot]), self.phi_ws[slot].numel(), st),
+                      "lf_phi_precompute_pp")
+            nat.check(lib.lf_lense_flow_pp(plan.handle, _ptr(self.d_f[slot]), code, _ptr(self.d_out[slot]), code,
+                                           _ptr(pp), m, int(n), int(direction), int(bool(adjoint)),
+                                           _ptr(self.ws[slot]), self.ws[slot].numel(), st), "lf_lense_flow_pp")
+            return
         nat.check(lib.lf_phi_precompute(plan.handle, _ptr(self.d_phi[slot]), nat.LF_PHI_MAP, m,
                                         _ptr(self.planes[slot]), md, _ptr(self.phi_ws[slot]),
                                         self.phi_ws[slot].numel(), st), "lf_phi_precompute")
-        code = nat.LF_F64 if self.io_dtype == torch.float64 else nat.LF_F32
         nat.check(lib.lf_lense_flow(plan.handle, _ptr(self.d_f[slot]), code, _ptr(self.d_out[slot]), code,
                                     _ptr(self.planes[slot]), m, int(n), int(direction), int(bool(adjoint)),
                                     _ptr(self.ws[slot]), self.ws[slot].numel(), st), "lf_lense_flow")
@@ -394,10 +486,10 @@ class HostPipeline:
     def __call__(self, f_host, phi_host, out_host, n=10, direction=FORWARD_LENSE, adjoint=False, check_det=True,
                  wait=True):
         plan, lib = self.plan, self.plan._lib
-        need = plan.workspace_bytes(self.cb, True, n)
-        for k in range(self.nslots):
-            if self.ws[k].numel() < need:
-                self.ws[k] = torch.empty(need, dtype=torch.uint8, device=plan.device)
+        if self.use_pp and n not in self.pp:
+            N = plan.nside
+            self.pp[n] = [torch.empty((self.cb, 2 * int(n) + 1, 2, N, N), dtype=torch.float32, device=plan.device)
+                          for _ in range(self.nslots)]
         cur = torch.cuda.current_stream(plan.device)
         streams = [self.s_in, self.s_out] + self.s_cmp
         for st in streams:

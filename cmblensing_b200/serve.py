@@ -96,8 +96,9 @@ class _LensSlot:
         self.d_f = torch.empty((cap, C, N, N), dtype=torch.float32, device=dev)
         self.d_phi = torch.empty((cap, N, N), dtype=torch.float64, device=dev)
         self.d_out = torch.empty_like(self.d_f)
-        self.planes = torch.empty((cap, 5, N, N), dtype=torch.float32, device=dev)
-        self.ws = torch.empty(max(self.plan.workspace_bytes(cap, True, n), 16), dtype=torch.uint8, device=dev)
+        # p = M(t)^-1 grad phi at the 2n+1 stage times, written by the phi precompute itself
+        self.pp = torch.empty((cap, 2 * n + 1, 2, N, N), dtype=torch.float32, device=dev)
+        self.ws = torch.empty(max(self.plan.workspace_bytes(cap, True), 16), dtype=torch.uint8, device=dev)
         self.phi_ws = torch.empty(max(self.plan.phi_workspace_bytes(cap), 16), dtype=torch.uint8, device=dev)
         self.md = torch.empty(cap, dtype=torch.int32, device=dev)
         self.stream = torch.cuda.Stream(dev, priority=priority)
@@ -111,12 +112,12 @@ class _LensSlot:
         p, lib = self.plan, self.plan._lib
         st = engine._stream_ptr(self.dev)
         nat.check(lib.lf_min_det_init(engine._ptr(self.md), b, st), "lf_min_det_init")
-        nat.check(lib.lf_phi_precompute(p.handle, engine._ptr(self.d_phi), nat.LF_PHI_MAP, b, engine._ptr(self.planes),
-                                        engine._ptr(self.md), engine._ptr(self.phi_ws), self.phi_ws.numel(), st),
-                  "lf_phi_precompute")
-        nat.check(lib.lf_lense_flow(p.handle, engine._ptr(self.d_f), nat.LF_F32, engine._ptr(self.d_out), nat.LF_F32,
-                                    engine._ptr(self.planes), b, self.n, self.direction, 0, engine._ptr(self.ws),
-                                    self.ws.numel(), st), "lf_lense_flow")
+        nat.check(lib.lf_phi_precompute_pp(p.handle, engine._ptr(self.d_phi), nat.LF_PHI_MAP, b, None,
+                                           engine._ptr(self.pp), self.n, engine._ptr(self.md), engine._ptr(self.phi_ws),
+                                           self.phi_ws.numel(), st), "lf_phi_precompute_pp")
+        nat.check(lib.lf_lense_flow_pp(p.handle, engine._ptr(self.d_f), nat.LF_F32, engine._ptr(self.d_out),
+                                       nat.LF_F32, engine._ptr(self.pp), b, self.n, self.direction, 0,
+                                       engine._ptr(self.ws), self.ws.numel(), st), "lf_lense_flow_pp")
 
     def launch(self, reqs):
         """Copy inputs in, run (graph replay or eager) and copy outputs out, all on this slot's stream."""
@@ -361,8 +362,8 @@ def run_alone(req):
     plan = engine.get_plan(req.nside, req.ncomp, req.theta_pix * ARCMIN, "f32")
     f = torch.as_tensor(np.asarray(req.f, dtype=np.float32), device="cuda").unsqueeze(0)
     phi = torch.as_tensor(np.asarray(req.phi, dtype=np.float64), device="cuda").unsqueeze(0)
-    planes = plan.phi_planes(phi, check_det=True)
-    return plan.lense_flow(f, planes, n=req.n, direction=nat_direction(req.kind))[0].cpu().numpy()
+    pp = plan.phi_pp(phi, req.n, check_det=True)
+    return plan.lense_flow_pp(f, pp, req.n, direction=nat_direction(req.kind))[0].cpu().numpy()
 
 
 def latency_summary(reqs):

@@ -86,6 +86,29 @@ int lf_phi_precompute(lf_plan_t plan, const void* phi, int phi_basis, int batch,
 int lf_min_det_init(int* min_det, int batch, void* stream);
 float lf_decode_min_det(int encoded);
 
+/* The phi precompute with the stage-time p planes formed in the same pass
+ * (float32 plans only; LF_ERR_BAD_DTYPE otherwise): pp receives
+ * p = M(t)^-1 grad(phi) (lense_flow.py:373-381, :398-415), computed in
+ * float64 from the float64 derivatives and stored float32, at the 2n+1 times
+ * k / (2n), k = 0..2n, ascending: [batch][2n+1][2][N][N] (lf_pp_bytes).  One
+ * set serves the forward, inverse and adjoint lens with n steps.  ``planes``
+ * (optional, NULL to skip) receives the five derivative planes as
+ * lf_phi_precompute writes them; ``min_det`` as in lf_phi_precompute.
+ * Workspace: lf_phi_workspace_bytes.  Replaces get_primal_derivatives
+ * (util.py:110-130) plus the per-RHS p computation of the reference. */
+size_t lf_pp_bytes(lf_plan_t plan, int batch, int nsteps);
+int lf_phi_precompute_pp(lf_plan_t plan, const void* phi, int phi_basis, int batch, void* planes, void* pp, int nsteps,
+                         int* min_det, void* workspace, size_t workspace_bytes, void* stream);
+/* lf_lense_flow reading precomputed p planes (from lf_phi_precompute_pp with
+ * the same nsteps) instead of forming them: float32 plans; workspace of
+ * lf_workspace_bytes.  Same results as lf_lense_flow on the p-plane path up
+ * to the p planes' rounding (formed here from float64 rather than float32
+ * derivatives).  Replaces lense_flow (lense_flow.py:289-352) as
+ * lf_lense_flow does. */
+int lf_lense_flow_pp(lf_plan_t plan, const void* f_in, int in_dtype, void* f_out, int out_dtype, const void* pp,
+                     int batch, int nsteps, int direction, int adjoint, void* workspace, size_t workspace_bytes,
+                     void* stream);
+
 /* LenseFlow: RK4 with ``nsteps`` fixed steps of df/dt = grad(phi)^T M^-1 grad f
  * (adjoint = 0) or df/dt = div(M^-1 grad(phi) f) (adjoint = 1), time running
  * 0 -> 1 iff (direction == +1) XOR adjoint.  Replaces lense_flow /

@@ -36,6 +36,13 @@ def test_column_and_p_plane_bytes():
     assert bench.p_plane_bytes_per_lens(7, P) == (20 + 8 * 15) * P
 
 
+def test_fused_phi_precompute_saves_the_plane_round_trip():
+    # the derivative planes (20 N^2 written, 20 N^2 read back) no longer cross HBM on the p-plane path
+    n = 7
+    assert bench.phi_pp_bytes_per_map(n, P) == (120 + 8 * 15) * P
+    assert 140 * P + bench.p_plane_bytes_per_lens(n, P) - bench.phi_pp_bytes_per_map(n, P) == 40 * P
+
+
 def test_stage1_bytes_match_the_stage_model():
     # the launch whose DRAM traffic the roofline line reports
     assert bench.stage1_bytes_per_map(2) == 48

@@ -386,8 +386,9 @@ def test_host_pipeline_matches_device_call(torch_cuda, B, chunks, sizes):
         oh.zero_()
         pipe(fh, ph, oh, n=7)
         torch.cuda.synchronize()
-    ref = plan.lense_flow(torch.as_tensor(f, device="cuda"), plan.phi_planes(torch.as_tensor(phis, device="cuda")),
-                          n=7)
+    # float32 plans: the pipeline forms the p planes in the phi precompute (phi_pp + lense_flow_pp)
+    ref = plan.lense_flow_pp(torch.as_tensor(f, device="cuda"), plan.phi_pp(torch.as_tensor(phis, device="cuda"), 7),
+                             7)
     assert torch.equal(oh, ref.cpu())
 
 
@@ -411,8 +412,8 @@ def test_host_pipeline_overlapped_calls(torch_cuda):
         pipe.wait()
         torch.cuda.synchronize()
         for k in range(2):
-            ref = plan.lense_flow(torch.as_tensor(f[k * 3:(k + 1) * 3], device="cuda"),
-                                  plan.phi_planes(torch.as_tensor(phis[k * 3:(k + 1) * 3], device="cuda")), n=7)
+            ref = plan.lense_flow_pp(torch.as_tensor(f[k * 3:(k + 1) * 3], device="cuda"),
+                                     plan.phi_pp(torch.as_tensor(phis[k * 3:(k + 1) * 3], device="cuda"), 7), 7)
             assert torch.equal(outs[k], ref.cpu()), (rep, k)
 
 
@@ -433,3 +434,50 @@ def test_host_pipeline_reports_singular_phi(torch_cuda):
          torch.empty(f.shape, dtype=torch.float64).pin_memory(), n=7, wait=False)
     with pytest.raises(nat.SingularMagnificationError):
         pipe.wait()
+
+
+# ------------------------------------------- p planes formed in the phi precompute
+@pytest.mark.parametrize("N,theta,C", [(64, 3.0, 1), (128, 3.0, 2), (256, 3.0, 3), (512, 2.0, 2), (1024, 2.0, 1)])
+def test_phi_pp_lens_matches_oracle_and_p_plane_path(torch_cuda, N, theta, C):
+    """lf_phi_precompute_pp + lf_lense_flow_pp: one ascending set of p planes serves the forward, inverse and
+    adjoint lens; every result matches the oracle (1e-5) and the lf_lense_flow p-plane path (1e-6: the p planes
+    differ only by being formed from float64 rather than float32 derivatives); the optional derivative planes
+    equal lf_phi_precompute's bit for bit, and the magnification minimum agrees."""
+    import torch
+    from cmblensing_b200 import engine
+    f, phis = _inputs(N, theta, C, B=2, seed0=50)
+    pw = R.pix_width_of(theta)
+    plan = engine.get_plan(N, C, pw)
+    ph = torch.as_tensor(phis, device="cuda")
+    planes = plan.phi_planes(ph)
+    md_planes = list(plan.last_min_det)
+    planes_pp = torch.empty_like(planes)
+    pp = plan.phi_pp(ph, 7, planes_out=planes_pp)
+    assert torch.equal(planes_pp, planes)
+    for a, b in zip(plan.last_min_det, md_planes):
+        assert abs(a - b) < 1e-6 * max(1.0, abs(b))
+    ft = torch.as_tensor(f, device="cuda", dtype=torch.float32)
+    cases = [(1, False), (-1, False), (1, True)] if N <= 512 else [(1, False)]
+    for direction, adjoint in cases:
+        got = plan.lense_flow_pp(ft, pp, 7, direction=direction, adjoint=adjoint)
+        ref_pp = plan.lense_flow(ft, planes, n=7, direction=direction, adjoint=adjoint)
+        assert float((got - ref_pp).norm() / ref_pp.norm()) < 1e-6
+        ref = _oracle(f[1], phis[1], pw, 7, direction, adjoint)
+        g = got[1].double().cpu().numpy()
+        for c in range(C):
+            assert rel_l2(g[c], ref[c]) < TOL32, (direction, adjoint, c)
+
+
+def test_phi_pp_reports_singular_phi_and_rejects_f64_plans(torch_cuda):
+    import torch
+    from cmblensing_b200 import _native as nat
+    from cmblensing_b200 import engine
+    from cmblensing_b200.simulate import gaussian_phi
+    phi = gaussian_phi(128, 3.0, seed=7, deflection_arcmin=2.5, spectrum="literal")
+    plan = engine.get_plan(128, 1, R.pix_width_of(3.0))
+    with pytest.raises(nat.SingularMagnificationError):
+        plan.phi_pp(torch.as_tensor(phi[None], device="cuda"), 7)
+    plan64 = engine.get_plan(128, 1, R.pix_width_of(3.0), "f64")
+    with pytest.raises(nat.LenseFlowError) as e:
+        plan64.phi_pp(torch.as_tensor(phi[None], device="cuda"), 7, check_det=False)
+    assert e.value.status == nat.LF_ERR_BAD_DTYPE

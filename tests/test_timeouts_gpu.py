@@ -94,5 +94,5 @@ def test_host_pipeline_raises_on_timeout(torch_cuda):
         engine.wait_timeouts(reset=True)
     pipe._pending.clear()
     pipe(fh, ph, oh, n=7)
-    ref = plan.lense_flow(torch.as_tensor(f, device="cuda"), plan.phi_planes(torch.as_tensor(phis, device="cuda")), n=7)
+    ref = plan.lense_flow_pp(torch.as_tensor(f, device="cuda"), plan.phi_pp(torch.as_tensor(phis, device="cuda"), 7), 7)
     assert rel_l2(oh.numpy(), ref.cpu().numpy()) == 0.0
