@@ -392,11 +392,11 @@ cudaError_t run_phi_n(const void* phi, int basis, int B, TO* planes, int* min_de
 
 // The phi precompute with the p planes formed in the derivative row pass (float32 plans):
 // rfft2 of phi (or its given spectrum), the three inverse column transforms of the five
-// derivatives, then k_phi_rows_c2r_pp over 4-row tiles of all five.
+// derivatives, then k_phi_rows_c2r_pp over 2-row tiles of all five.
 template <int N>
 cudaError_t run_phi_pp_n(const void* phi, int basis, int B, float* planes, float* pp, int K, int* min_det, void* ws,
                          const double2* tw64, double kbase, cudaStream_t st) {
-  constexpr int LINES = 8, PL = 4;
+  constexpr int LINES = 8, PL = 2;
   constexpr int NT = Geo<double>::nt(N);
   constexpr int H = N / 2;
   double2* spec = reinterpret_cast<double2*>(ws);

@@ -1094,17 +1094,20 @@ __global__ void k_min_det(const T* __restrict__ planes, long P, int* __restrict_
 // ============================ fused: derivative rows -> p planes at the stage times
 // The inverse real row transforms of all five derivative spectra of LINES
 // rows (as k_phi_rows_c2r, float64), and in the same block, from the five
-// derivatives of each pixel held in float64: p = M(t)^-1 grad(phi)
-// (lense_flow.py:373-381, :398-415) at the K = 2n+1 times k / (2n), stored
+// derivatives of each pixel: p = M(t)^-1 grad(phi) (lense_flow.py:373-381,
+// :398-415) at the K = 2n+1 times k / (2n), in float32 arithmetic and stored
 // float32 ascending in time ([B][K][2][N][N]), and the per-map minimum of
-// det(I + t grad grad phi) over pixels and t in [0, 1] (as k_min_det).  The
+// det(I + t grad grad phi) over pixels and t in [0, 1] (float64, as
+// k_min_det).  The
 // five derivative planes are written only when ``planes`` is non-null, so
 // the forward lens's p planes no longer round-trip them through HBM.
-// grid: x = row tile, y = map.  NT: one first-pass butterfly per thread (a warp multiple).
-__host__ __device__ constexpr int pp_threads(int n) { return n <= 64 ? 96 : (n == 128 ? 160 : (n <= 512 ? 320 : 512)); }
+// grid: x = row tile, y = map.  NT: about one first-pass butterfly per thread (a warp multiple); 2-row
+// tiles, four blocks per SM (measured against 4-row tiles at two: 1.142 vs 1.153 ms of phi precompute per
+// 64-map 512^2 step).
+__host__ __device__ constexpr int pp_threads(int n) { return n <= 64 ? 64 : (n == 128 ? 96 : (n <= 512 ? 160 : 320)); }
 
 template <int N, int LINES, int NT>
-__global__ void __launch_bounds__(NT, N == 1024 ? 1 : 2) k_phi_rows_c2r_pp(const double2* __restrict__ packed, float* __restrict__ planes,
+__global__ void __launch_bounds__(NT, N == 1024 ? 2 : 4) k_phi_rows_c2r_pp(const double2* __restrict__ packed, float* __restrict__ planes,
                                                          float* __restrict__ pp, int K, int* __restrict__ min_det,
                                                          const double2* __restrict__ twN) {
   constexpr int H = N / 2;
@@ -1160,12 +1163,19 @@ __global__ void __launch_bounds__(NT, N == 1024 ? 1 : 2) k_phi_rows_c2r_pp(const
       best = fmin(best, dm);
     }
     float* out = pp + map * (long)K * 2 * P + o;
+    // p in float32 arithmetic, as the RK4 right-hand side that reads it (float64 here kept the FP64 pipe
+    // busy for no accuracy the float32 planes could hold: 0.05 ms more per 64-map step)
+    float df[5][4];
+#pragma unroll
+    for (int j = 0; j < 5; ++j)
+#pragma unroll
+      for (int q = 0; q < 4; ++q) df[j][q] = float(d[j][q]);
 #pragma unroll 1
     for (int k = 0; k < K; ++k) {
-      const double t = double(k) * inv2n;
-      double ox[4], oy[4];
+      const float t = float(double(k) * inv2n);
+      float ox[4], oy[4];
 #pragma unroll
-      for (int q = 0; q < 4; ++q) p_vector<double>(d[0][q], d[1][q], d[2][q], d[3][q], d[4][q], t, ox[q], oy[q]);
+      for (int q = 0; q < 4; ++q) p_vector<float>(df[0][q], df[1][q], df[2][q], df[3][q], df[4][q], t, ox[q], oy[q]);
       *reinterpret_cast<float4*>(out + (2 * k) * P) =
           make_float4(float(ox[0]), float(ox[1]), float(ox[2]), float(ox[3]));
       *reinterpret_cast<float4*>(out + (2 * k + 1) * P) =

@@ -89,7 +89,7 @@ float lf_decode_min_det(int encoded);
 /* The phi precompute with the stage-time p planes formed in the same pass
  * (float32 plans only; LF_ERR_BAD_DTYPE otherwise): pp receives
  * p = M(t)^-1 grad(phi) (lense_flow.py:373-381, :398-415), computed in
- * float64 from the float64 derivatives and stored float32, at the 2n+1 times
+ * float32 (the RK4 arithmetic) from the float64 derivatives, at the 2n+1 times
  * k / (2n), k = 0..2n, ascending: [batch][2n+1][2][N][N] (lf_pp_bytes).  One
  * set serves the forward, inverse and adjoint lens with n steps.  ``planes``
  * (optional, NULL to skip) receives the five derivative planes as
@@ -102,8 +102,8 @@ int lf_phi_precompute_pp(lf_plan_t plan, const void* phi, int phi_basis, int bat
 /* lf_lense_flow reading precomputed p planes (from lf_phi_precompute_pp with
  * the same nsteps) instead of forming them: float32 plans; workspace of
  * lf_workspace_bytes.  Same results as lf_lense_flow on the p-plane path up
- * to the p planes' rounding (formed here from float64 rather than float32
- * derivatives).  Replaces lense_flow (lense_flow.py:289-352) as
+ * to the p planes' rounding (float32 arithmetic on float64 derivatives here,
+ * float64 arithmetic on float32 derivative planes there).  Replaces lense_flow (lense_flow.py:289-352) as
  * lf_lense_flow does. */
 int lf_lense_flow_pp(lf_plan_t plan, const void* f_in, int in_dtype, void* f_out, int out_dtype, const void* pp,
                      int batch, int nsteps, int direction, int adjoint, void* workspace, size_t workspace_bytes,

@@ -441,7 +441,8 @@ def test_host_pipeline_reports_singular_phi(torch_cuda):
 def test_phi_pp_lens_matches_oracle_and_p_plane_path(torch_cuda, N, theta, C):
     """lf_phi_precompute_pp + lf_lense_flow_pp: one ascending set of p planes serves the forward, inverse and
     adjoint lens; every result matches the oracle (1e-5) and the lf_lense_flow p-plane path (1e-6: the p planes
-    differ only by being formed from float64 rather than float32 derivatives); the optional derivative planes
+    differ only in rounding: float32 arithmetic on float64 derivatives there, float64 arithmetic on float32
+    planes here); the optional derivative planes
     equal lf_phi_precompute's bit for bit, and the magnification minimum agrees."""
     import torch
     from cmblensing_b200 import engine
