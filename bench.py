@@ -74,6 +74,10 @@ def workload_config(a):
             "phi_spectrum": "1/[l^2 (l+1)^2 (1+(l/60)^2)], 2.5' rms deflection (well-posed reading)",
             "fields": "QU from E ~ l^-2 exp(-(l/2000)^2), 5 uK rms, B=0" if a.ncomp == 2 else "T",
             "l2": "inputs larger than L2 (working set ~1.4 GB per GPU), no flush",
+            "magnification_check": "det(I + t grad grad phi) > 0 checked once before the timed region; "
+                                   "the e2e leg checks every call",
+            "phi_path": "float64 phi precompute writing p = M(t)^-1 grad phi at the 2n+1 stage times "
+                        "(lf_phi_precompute_pp), then lf_lense_flow_pp",
             "parallelism": f"replicas x{a.gpus} (independent batches, no collective)"}
 
 
@@ -732,7 +736,9 @@ def main():
                                       "rel_l2_fp32_vs_fp64": rel}
 
     # ---------------------------------------------------- configs 2 and 3
-    if rank == 0 and not a.no_workloads:
+    # the 1-GPU legs (gradient, Wiener filter, serving) run only in single-process runs: under torchrun the
+    # other ranks would idle at the closing barrier meanwhile
+    if rank == 0 and world == 1 and not a.no_workloads:
         for key, fn in (("gradient", run_gradient), ("wf", run_wf)):
             try:
                 result[key] = fn(a, dev)
@@ -740,7 +746,7 @@ def main():
                 result[key] = {"error": repr(e)}
 
     # ---------------------------------------------------- serving
-    if rank == 0 and (a.serving_seconds > 0 or a.serving_requests > 0):
+    if rank == 0 and world == 1 and (a.serving_seconds > 0 or a.serving_requests > 0):
         try:
             result["serving"] = run_serving(a)
         except Exception as e:  # the headline numbers stand on their own

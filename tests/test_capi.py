@@ -57,6 +57,20 @@ def test_null_plan_calls_return_status(lib):
     assert lib.lf_plan_destroy(None) == nat.LF_OK
 
 
+def test_new_entry_points_validate_before_touching_the_device(lib):
+    """Null plans and bad arguments come back as status codes (no device work)."""
+    assert lib.lf_pp_bytes(None, 4, 7) == 0
+    assert lib.lf_vjp_ckpt_workspace_bytes(None, 4, 7) == 0
+    assert lib.lf_phi_precompute_pp(None, None, 0, 1, None, None, 7, None, None, 0, None) == nat.LF_ERR_BAD_ARG
+    assert lib.lf_lense_flow_pp(None, None, 0, None, 0, None, 1, 7, 1, 0, None, 0, None) == nat.LF_ERR_BAD_ARG
+    assert lib.lf_lense_flow_vjp_ckpt(None, None, None, 0, None, 1, 7, 1, None, None, None, 0, None, 0,
+                                      None) == nat.LF_ERR_BAD_ARG
+    # per-mode products: bad shapes and misaligned pointers are refused
+    assert lib.lf_modes_apply(None, 0, 1, None, None, None, 1, 4, 10, 1.0, 0.0, None) == nat.LF_ERR_BAD_SHAPE
+    assert lib.lf_modes_apply(None, 0, 1, None, None, None, 1, 1, 10, 1.0, 0.0, None) == nat.LF_ERR_BAD_ARG
+    assert lib.lf_modes_apply(None, 0, 1, None, None, None, 0, 1, 10, 1.0, 0.0, None) == nat.LF_OK
+
+
 def test_timeout_status_without_a_plan(lib):
     """No plan, no recorded timeout: the status word reads OK without touching the device."""
     assert lib.lf_timeout_status() == nat.LF_OK

@@ -482,3 +482,36 @@ def test_phi_pp_reports_singular_phi_and_rejects_f64_plans(torch_cuda):
     with pytest.raises(nat.LenseFlowError) as e:
         plan64.phi_pp(torch.as_tensor(phi[None], device="cuda"), 7, check_det=False)
     assert e.value.status == nat.LF_ERR_BAD_DTYPE
+
+
+def test_phi_pp_fourier_basis_equals_map_basis(torch_cuda):
+    """A Fourier phi (the rfft2 of a real map) and the map itself give the same p planes and lens."""
+    import torch
+    from cmblensing_b200 import engine
+    f, phis = _inputs(128, 3.0, 2, B=2, seed0=60)
+    plan = engine.get_plan(128, 2, R.pix_width_of(3.0))
+    pp_map = plan.phi_pp(torch.as_tensor(phis, device="cuda"), 7)
+    pp_four = plan.phi_pp(torch.as_tensor(np.fft.rfft2(phis), device="cuda"), 7)
+    assert float((pp_map - pp_four).norm() / pp_map.norm()) < 1e-6
+    ft = torch.as_tensor(f, device="cuda", dtype=torch.float32)
+    a = plan.lense_flow_pp(ft, pp_map, 7)
+    b = plan.lense_flow_pp(ft, pp_four, 7)
+    assert float((a - b).norm() / a.norm()) < 1e-6
+
+
+def test_host_pipeline_float64_plan(torch_cuda):
+    """A float64 plan's pipeline keeps the derivative-plane path and equals the device call bit for bit."""
+    import torch
+    from cmblensing_b200 import engine
+    f, phis = _inputs(64, 3.0, 1, B=4, seed0=61)
+    plan = engine.get_plan(64, 1, R.pix_width_of(3.0), "f64")
+    pipe = engine.HostPipeline(plan, 4, chunks=2)
+    assert not pipe.use_pp
+    fh = torch.from_numpy(f).pin_memory()
+    ph = torch.from_numpy(phis).pin_memory()
+    oh = torch.empty_like(fh).pin_memory()
+    for _ in range(3):  # eager, capture, replay
+        pipe(fh, ph, oh, n=7)
+    ref = plan.lense_flow(torch.as_tensor(f, device="cuda"), plan.phi_planes(torch.as_tensor(phis, device="cuda")),
+                          n=7)
+    assert torch.equal(oh, ref.cpu())
