@@ -695,5 +695,24 @@ def lense_flow_batch(f, phi, pix_width, n=10, direction=FORWARD_LENSE, adjoint=F
     return plan.lense_flow(f, planes, n=n, direction=direction, adjoint=adjoint)
 
 
+def lense_flow_dlpack(f, phi, pix_width, n=10, direction=FORWARD_LENSE, adjoint=False, precision="f32"):
+    """Zero-copy LenseFlow on arrays of any DLPack producer (CuPy, JAX, numba, torch ...).
+
+    ``f`` [B,C,N,N] and ``phi`` [B,N,N] (map) or [B,N,N/2+1] (Fourier) are
+    imported with ``torch.from_dlpack`` -- device arrays are used in place --
+    lensed on the engine, and the result is returned as a torch tensor, which
+    is itself a DLPack producer (``jax.dlpack.from_dlpack(out)``,
+    ``cupy.from_dlpack(out)``).  Host arrays are copied to the current device
+    first."""
+    ft = torch.from_dlpack(f)
+    pt = torch.from_dlpack(phi)
+    dev = ft.device if ft.is_cuda else torch.device("cuda", torch.cuda.current_device())
+    ft = ft.to(dev)
+    pt = pt.to(dev)
+    if ft.dtype not in (torch.float32, torch.float64):
+        ft = ft.to(torch.float64)
+    return lense_flow_batch(ft, pt, pix_width, n=n, direction=direction, adjoint=adjoint, precision=precision)
+
+
 __all__ = ["Plan", "HostPipeline", "LenseFlowFunction", "get_plan", "lense_flow_ad", "lense_flow_batch",
-           "FORWARD_LENSE", "INVERSE_LENSE"]
+           "lense_flow_dlpack", "FORWARD_LENSE", "INVERSE_LENSE"]

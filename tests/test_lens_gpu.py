@@ -515,3 +515,18 @@ def test_host_pipeline_float64_plan(torch_cuda):
     ref = plan.lense_flow(torch.as_tensor(f, device="cuda"), plan.phi_planes(torch.as_tensor(phis, device="cuda")),
                           n=7)
     assert torch.equal(oh, ref.cpu())
+
+
+def test_dlpack_entry_point(torch_cuda):
+    """engine.lense_flow_dlpack takes any DLPack producer (here a numpy host array and a torch CUDA tensor)
+    and returns a DLPack-capable tensor equal to the plain device call."""
+    import torch
+    from cmblensing_b200 import engine
+    f, phis = _inputs(64, 3.0, 2, B=2, seed0=70)
+    pw = R.pix_width_of(3.0)
+    out = engine.lense_flow_dlpack(np.ascontiguousarray(f), torch.as_tensor(phis, device="cuda"), pw, n=7)
+    assert out.is_cuda and hasattr(out, "__dlpack__")
+    ref = engine.lense_flow_batch(torch.as_tensor(f, device="cuda"), torch.as_tensor(phis, device="cuda"), pw, n=7)
+    assert torch.equal(out, ref)
+    back = torch.from_dlpack(out.__dlpack__())
+    assert back.data_ptr() == out.data_ptr()
