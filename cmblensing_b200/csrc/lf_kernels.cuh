@@ -1163,19 +1163,34 @@ __global__ void __launch_bounds__(NT, N == 1024 ? 2 : 4) k_phi_rows_c2r_pp(const
       best = fmin(best, dm);
     }
     float* out = pp + map * (long)K * 2 * P + o;
-    // p in float32 arithmetic, as the RK4 right-hand side that reads it (float64 here kept the FP64 pipe
-    // busy for no accuracy the float32 planes could hold: 0.05 ms more per 64-map step)
-    float df[5][4];
+    // p = M(t)^-1 grad phi through the adjugate of the symmetric 2x2 M = I + t H (H = grad grad phi):
+    //   p_x = (phi_x + t (H_yy phi_x - H_xy phi_y)) / D,  p_y = (phi_y + t (H_xx phi_y - H_xy phi_x)) / D,
+    //   D = det M = 1 + t (H_xx + H_yy) + t^2 (H_xx H_yy - H_xy^2).
+    // The time-independent coefficients are formed once per pixel in float64; each time then costs two
+    // FMAs for D, one reciprocal and four FMA/multiplies in float32 (the RK4 right-hand side that reads
+    // the planes is float32).  The reference's det + 1e-12 (lense_flow.py:408-411) is below float32
+    // resolution for D >= 0.2 and is not added.
+    float gx[4], gy[4], bx[4], by[4], lt[4], qt[4];
 #pragma unroll
-    for (int j = 0; j < 5; ++j)
-#pragma unroll
-      for (int q = 0; q < 4; ++q) df[j][q] = float(d[j][q]);
+    for (int q = 0; q < 4; ++q) {
+      const double A = d[2][q], Bx = d[3][q], Cc = d[4][q];
+      gx[q] = float(d[0][q]);
+      gy[q] = float(d[1][q]);
+      bx[q] = float(Cc * d[0][q] - Bx * d[1][q]);
+      by[q] = float(A * d[1][q] - Bx * d[0][q]);
+      lt[q] = float(A + Cc);
+      qt[q] = float(A * Cc - Bx * Bx);
+    }
 #pragma unroll 1
     for (int k = 0; k < K; ++k) {
       const float t = float(double(k) * inv2n);
       float ox[4], oy[4];
 #pragma unroll
-      for (int q = 0; q < 4; ++q) p_vector<float>(df[0][q], df[1][q], df[2][q], df[3][q], df[4][q], t, ox[q], oy[q]);
+      for (int q = 0; q < 4; ++q) {
+        const float r = __frcp_rn(fmaf(t, fmaf(t, qt[q], lt[q]), 1.0f));
+        ox[q] = fmaf(t, bx[q], gx[q]) * r;
+        oy[q] = fmaf(t, by[q], gy[q]) * r;
+      }
       *reinterpret_cast<float4*>(out + (2 * k) * P) =
           make_float4(float(ox[0]), float(ox[1]), float(ox[2]), float(ox[3]));
       *reinterpret_cast<float4*>(out + (2 * k + 1) * P) =
