@@ -33,45 +33,49 @@
 
 namespace lf {
 
+// Pure-arithmetic helpers and the register DFTs compile for the host as well
+// (their unit test runs on the CPU).
+#define LF_HD __host__ __device__ __forceinline__
+
 template <typename T> struct V2;
 template <> struct V2<float> { using type = float2; };
 template <> struct V2<double> { using type = double2; };
 template <typename T> using c2 = typename V2<T>::type;
 
-template <typename T> __device__ __forceinline__ c2<T> mk(T x, T y) { c2<T> r; r.x = x; r.y = y; return r; }
-template <typename T> __device__ __forceinline__ c2<T> cadd(c2<T> a, c2<T> b) { return mk<T>(a.x + b.x, a.y + b.y); }
-template <typename T> __device__ __forceinline__ c2<T> csub(c2<T> a, c2<T> b) { return mk<T>(a.x - b.x, a.y - b.y); }
-template <typename T> __device__ __forceinline__ c2<T> cmul(c2<T> a, c2<T> b) {
+template <typename T> LF_HD c2<T> mk(T x, T y) { c2<T> r; r.x = x; r.y = y; return r; }
+template <typename T> LF_HD c2<T> cadd(c2<T> a, c2<T> b) { return mk<T>(a.x + b.x, a.y + b.y); }
+template <typename T> LF_HD c2<T> csub(c2<T> a, c2<T> b) { return mk<T>(a.x - b.x, a.y - b.y); }
+template <typename T> LF_HD c2<T> cmul(c2<T> a, c2<T> b) {
   return mk<T>(a.x * b.x - a.y * b.y, a.x * b.y + a.y * b.x);
 }
 // a * conj(b)
-template <typename T> __device__ __forceinline__ c2<T> cmulc(c2<T> a, c2<T> b) {
+template <typename T> LF_HD c2<T> cmulc(c2<T> a, c2<T> b) {
   return mk<T>(a.x * b.x + a.y * b.y, a.y * b.x - a.x * b.y);
 }
-template <typename T> __device__ __forceinline__ c2<T> cconj(c2<T> a) { return mk<T>(a.x, -a.y); }
-template <typename T> __device__ __forceinline__ c2<T> cscale(c2<T> a, T s) { return mk<T>(a.x * s, a.y * s); }
+template <typename T> LF_HD c2<T> cconj(c2<T> a) { return mk<T>(a.x, -a.y); }
+template <typename T> LF_HD c2<T> cscale(c2<T> a, T s) { return mk<T>(a.x * s, a.y * s); }
 // multiply by i
-template <typename T> __device__ __forceinline__ c2<T> cmul_i(c2<T> a) { return mk<T>(-a.y, a.x); }
+template <typename T> LF_HD c2<T> cmul_i(c2<T> a) { return mk<T>(-a.y, a.x); }
 
 // Twiddle multiply by exp(-+2 pi i e/NTAB): forward uses tw[e], inverse conj(tw[e]).
-template <typename T, bool INV> __device__ __forceinline__ c2<T> twmul(c2<T> a, c2<T> w) {
+template <typename T, bool INV> LF_HD c2<T> twmul(c2<T> a, c2<T> w) {
   return INV ? cmulc<T>(a, w) : cmul<T>(a, w);
 }
 
 // x * (-i) for the forward transform, x * (+i) for the inverse.
-template <typename T, bool INV> __device__ __forceinline__ c2<T> rot90(c2<T> a) {
+template <typename T, bool INV> LF_HD c2<T> rot90(c2<T> a) {
   return INV ? mk<T>(-a.y, a.x) : mk<T>(a.y, -a.x);
 }
 
 // ----------------------------------------------------------- small DFTs
 // In-place, natural order in and out, unnormalised; forward kernel e^{-2 pi i jk/R}.
-template <typename T, bool INV> __device__ __forceinline__ void dft2(c2<T>* a) {
+template <typename T, bool INV> LF_HD void dft2(c2<T>* a) {
   c2<T> t = a[0];
   a[0] = cadd<T>(t, a[1]);
   a[1] = csub<T>(t, a[1]);
 }
 
-template <typename T, bool INV> __device__ __forceinline__ void dft4(c2<T>* a) {
+template <typename T, bool INV> LF_HD void dft4(c2<T>* a) {
   c2<T> t0 = cadd<T>(a[0], a[2]), t1 = csub<T>(a[0], a[2]);
   c2<T> t2 = cadd<T>(a[1], a[3]), t3 = rot90<T, INV>(csub<T>(a[1], a[3]));
   a[0] = cadd<T>(t0, t2);
@@ -85,7 +89,7 @@ template <typename T, bool INV> __device__ __forceinline__ void dft4(c2<T>* a) {
 #define LF_C22 0.92387953251128675613
 #define LF_S22 0.38268343236508977173
 
-template <typename T, bool INV> __device__ __forceinline__ void dft8(c2<T>* a) {
+template <typename T, bool INV> LF_HD void dft8(c2<T>* a) {
   c2<T> e[4] = {a[0], a[2], a[4], a[6]};
   c2<T> o[4] = {a[1], a[3], a[5], a[7]};
   dft4<T, INV>(e);
@@ -108,7 +112,28 @@ template <typename T, bool INV> __device__ __forceinline__ void dft8(c2<T>* a) {
   a[7] = csub<T>(e[3], o3);
 }
 
-template <typename T, bool INV> __device__ __forceinline__ void dft16(c2<T>* a) {
+// a <- a + w b, b <- a - w b for a constant twiddle w = (wr, wi), with FMAs: w b is written as
+// wr (1 + i wi/wr) b when |wr| >= |wi|, else wi (wr/wi + i) b, so the scaled b costs two FMAs and
+// each output two more (six instructions instead of eight for a multiply, then an add and a subtract).
+template <typename T> LF_HD void bfly_w(c2<T>& a, c2<T>& b, double wr, double wi) {
+  c2<T> u;
+  T f;
+  if (wr * wr >= wi * wi) {
+    const T t = T(wi / wr);
+    u = mk<T>(b.x - t * b.y, b.y + t * b.x);
+    f = T(wr);
+  } else {
+    const T t = T(wr / wi);
+    u = mk<T>(t * b.x - b.y, t * b.y + b.x);
+    f = T(wi);
+  }
+  const c2<T> a0 = a;
+  a = mk<T>(a0.x + f * u.x, a0.y + f * u.y);
+  b = mk<T>(a0.x - f * u.x, a0.y - f * u.y);
+}
+
+// Radix-2 split into two 8-point DFTs: X[k] = E[k] + W16^k O[k], X[k+8] = E[k] - W16^k O[k].
+template <typename T, bool INV> LF_HD void dft16(c2<T>* a) {
   c2<T> e[8], o[8];
 #pragma unroll
   for (int i = 0; i < 8; ++i) {
@@ -118,14 +143,19 @@ template <typename T, bool INV> __device__ __forceinline__ void dft16(c2<T>* a) 
   dft8<T, INV>(e);
   dft8<T, INV>(o);
   // W16^k forward = (cos(pi k/8), -sin(pi k/8)), k = 0..7
-  const T wr[8] = {T(1), T(LF_C22), T(LF_C45), T(LF_S22), T(0), T(-LF_S22), T(-LF_C45), T(-LF_C22)};
-  const T wi[8] = {T(0), T(-LF_S22), T(-LF_C45), T(-LF_C22), T(-1), T(-LF_C22), T(-LF_C45), T(-LF_S22)};
+  const double wr[8] = {1.0, LF_C22, LF_C45, LF_S22, 0.0, -LF_S22, -LF_C45, -LF_C22};
+  const double ws[8] = {0.0, LF_S22, LF_C45, LF_C22, 1.0, LF_C22, LF_C45, LF_S22};
 #pragma unroll
   for (int k = 0; k < 8; ++k) {
-    c2<T> w = mk<T>(wr[k], INV ? -wi[k] : wi[k]);
-    c2<T> t = (k == 0) ? o[k] : (k == 4 ? rot90<T, INV>(o[k]) : cmul<T>(o[k], w));
-    a[k] = cadd<T>(e[k], t);
-    a[k + 8] = csub<T>(e[k], t);
+    if (k == 0 || k == 4) {
+      const c2<T> t = (k == 0) ? o[k] : rot90<T, INV>(o[k]);
+      a[k] = cadd<T>(e[k], t);
+      a[k + 8] = csub<T>(e[k], t);
+    } else {
+      bfly_w<T>(e[k], o[k], wr[k], INV ? ws[k] : -ws[k]);
+      a[k] = e[k];
+      a[k + 8] = o[k];
+    }
   }
 }
 
@@ -136,7 +166,7 @@ template <typename T, bool INV> __device__ __forceinline__ void dft16(c2<T>* a) 
 #define LF_S33 0.55557023301960222474
 
 // Radix-2 split into two 16-point DFTs: X[k] = E[k] + W32^k O[k], X[k+16] = E[k] - W32^k O[k].
-template <typename T, bool INV> __device__ __forceinline__ void dft32(c2<T>* a) {
+template <typename T, bool INV> LF_HD void dft32(c2<T>* a) {
   c2<T> e[16], o[16];
 #pragma unroll
   for (int i = 0; i < 16; ++i) {
@@ -146,20 +176,25 @@ template <typename T, bool INV> __device__ __forceinline__ void dft32(c2<T>* a) 
   dft16<T, INV>(e);
   dft16<T, INV>(o);
   // W32^k forward = (cos(pi k/16), -sin(pi k/16)), k = 0..15
-  const T wr[16] = {T(1),       T(LF_C11),  T(LF_C22),  T(LF_C33),  T(LF_C45), T(LF_S33),  T(LF_S22),  T(LF_S11),
-                    T(0),       T(-LF_S11), T(-LF_S22), T(-LF_S33), T(-LF_C45), T(-LF_C33), T(-LF_C22), T(-LF_C11)};
-  const T ws[16] = {T(0),      T(LF_S11), T(LF_S22), T(LF_S33), T(LF_C45), T(LF_C33), T(LF_C22), T(LF_C11),
-                    T(1),      T(LF_C11), T(LF_C22), T(LF_C33), T(LF_C45), T(LF_S33), T(LF_S22), T(LF_S11)};
+  const double wr[16] = {1.0,     LF_C11,  LF_C22,  LF_C33,  LF_C45,  LF_S33,  LF_S22,  LF_S11,
+                         0.0,     -LF_S11, -LF_S22, -LF_S33, -LF_C45, -LF_C33, -LF_C22, -LF_C11};
+  const double ws[16] = {0.0,    LF_S11, LF_S22, LF_S33, LF_C45, LF_C33, LF_C22, LF_C11,
+                         1.0,    LF_C11, LF_C22, LF_C33, LF_C45, LF_S33, LF_S22, LF_S11};
 #pragma unroll
   for (int k = 0; k < 16; ++k) {
-    const c2<T> w = mk<T>(wr[k], INV ? ws[k] : -ws[k]);
-    const c2<T> t = (k == 0) ? o[k] : (k == 8 ? rot90<T, INV>(o[k]) : cmul<T>(o[k], w));
-    a[k] = cadd<T>(e[k], t);
-    a[k + 16] = csub<T>(e[k], t);
+    if (k == 0 || k == 8) {
+      const c2<T> t = (k == 0) ? o[k] : rot90<T, INV>(o[k]);
+      a[k] = cadd<T>(e[k], t);
+      a[k + 16] = csub<T>(e[k], t);
+    } else {
+      bfly_w<T>(e[k], o[k], wr[k], INV ? ws[k] : -ws[k]);
+      a[k] = e[k];
+      a[k + 16] = o[k];
+    }
   }
 }
 
-template <int R, typename T, bool INV> __device__ __forceinline__ void dft(c2<T>* a) {
+template <int R, typename T, bool INV> LF_HD void dft(c2<T>* a) {
   if constexpr (R == 2) dft2<T, INV>(a);
   else if constexpr (R == 4) dft4<T, INV>(a);
   else if constexpr (R == 8) dft8<T, INV>(a);
