@@ -335,7 +335,7 @@ class Plan:
         return ms.value, n.value
 
 
-def chunk_schedule(batch, chunks=16, chunk_sizes=None):
+def chunk_schedule(batch, chunks=8, chunk_sizes=None):
     """Chunk sizes of a HostPipeline call: ``chunk_sizes`` as given (positive, summing to ``batch``), else
     ``chunks`` near-equal chunks (the last may be shorter)."""
     if chunk_sizes is None:
@@ -367,7 +367,11 @@ class HostPipeline:
     512^2 QU maps with float64 host I/O: 4,528 maps/s on one stream, 5,600
     with two compute streams, 6,411 with graphs, 7,240 with consecutive calls
     queued (``wait=False``) so that each call's fill and drain overlap its
-    neighbours (same outputs bit for bit).
+    neighbours (same outputs bit for bit).  With calls queued, the neighbours
+    also hide a larger chunk's longer fill, and 8 chunks of 8 maps (the
+    default) beat 16 chunks of 4 (per-map compute is cheaper at 8 maps):
+    7,818-7,940 against 7,415-7,424 maps/s in two sweeps on one box (4
+    chunks 7,770-7,844, 32 chunks 6,133-6,136).
     The magnification minima are read back after the last chunk; a call
     whose phi is singular raises SingularMagnificationError (its outputs are
     then meaningless).  ``wait=False`` returns once the call is queued: the
@@ -380,7 +384,7 @@ class HostPipeline:
     is known).
     """
 
-    def __init__(self, plan, batch, io_dtype=torch.float64, chunks=16, compute_streams=2, slots=4,
+    def __init__(self, plan, batch, io_dtype=torch.float64, chunks=8, compute_streams=2, slots=4,
                  use_graphs=True, chunk_sizes=None):
         self.plan = plan
         N, C = plan.nside, plan.ncomp
