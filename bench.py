@@ -513,8 +513,13 @@ def run_serving(a):
         i = int(rng.integers(2))
         return Request(str(kind), N, C, th, f=f[i], phi=ph[i], n=7)
 
-    # warm every shape once (graph capture, plans, kernel attributes) outside the measurement
-    srv = Server(max_batch=16).start()
+    # every lens shape's slots and batch-bucket graphs before the server starts, then one request of every
+    # shape (plans, kernel attributes, the Wiener-filter path), all outside the measurement
+    srv = Server(max_batch=16)
+    for N, th in SERVE_SIZES.items():
+        for C in (1, 2):
+            srv.prepare(N, C, th)
+    srv.start()
     warm = [srv.submit(Request(k, N, C, th, f=pools[(N, C)][0][0], phi=pools[(N, C)][1][0], n=7))
             for N, th in SERVE_SIZES.items() for C in (1, 2) for k in ("lens", "delens")]
     warm += [srv.submit(Request("wf", N, C, th, problem=wf[(N, C)], n=7, wf_kwargs=wf_kw))

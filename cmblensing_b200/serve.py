@@ -119,28 +119,34 @@ class _LensSlot:
                                        nat.LF_F32, engine._ptr(self.pp), b, self.n, self.direction, 0,
                                        engine._ptr(self.ws), self.ws.numel(), st), "lf_lense_flow_pp")
 
+    def _graph(self, bb):
+        """The captured graph for batch bucket ``bb`` (captured on first use, on this slot's stream)."""
+        g = self.graphs.get(bb)
+        if g is None:
+            with torch.cuda.stream(self.stream):
+                self._body(bb)  # eager warm-up: kernel attributes are set outside the capture
+                # thread-local capture without a device-wide synchronisation: Wiener-filter
+                # workers keep running, and capturing, on their own threads
+                g = engine.capture_graph(lambda: self._body(bb), stream=self.stream)
+            self.graphs[bb] = g
+        return g
+
     def launch(self, reqs):
         """Copy inputs in, run (graph replay or eager) and copy outputs out, all on this slot's stream."""
         b = len(reqs)
         self.reqs = reqs
         self.busy = True
         for i, r in enumerate(reqs):
-            self.h_f[i].copy_(torch.from_numpy(np.asarray(r.f, dtype=np.float32)))
-            self.h_phi[i].copy_(torch.from_numpy(np.asarray(r.phi, dtype=np.float64)))
+            # torch converts float64 -> float32 inside the copy, multi-threaded and without the GIL
+            self.h_f[i].copy_(torch.from_numpy(np.ascontiguousarray(r.f)))
+            self.h_phi[i].copy_(torch.from_numpy(np.ascontiguousarray(r.phi)))
         with torch.cuda.stream(self.stream):
             self.d_f[:b].copy_(self.h_f[:b], non_blocking=True)
             self.d_phi[:b].copy_(self.h_phi[:b], non_blocking=True)
             bb = _bucket(b) if self.use_graphs else b
             bb = min(bb, self.cap)
             if self.use_graphs:
-                g = self.graphs.get(bb)
-                if g is None:
-                    self._body(bb)  # eager warm-up: kernel attributes are set outside the capture
-                    # thread-local capture without a device-wide synchronisation: Wiener-filter
-                    # workers keep running, and capturing, on their own threads
-                    g = engine.capture_graph(lambda: self._body(bb), stream=self.stream)
-                    self.graphs[bb] = g
-                g.replay()
+                self._graph(bb).replay()
             else:
                 self._body(b)
             self.h_out[:b].copy_(self.d_out[:b], non_blocking=True)
@@ -221,6 +227,32 @@ class Server:
             self.wf_cond.notify_all()
         for t in self._wf_threads:
             t.join()
+
+    def prepare(self, nside, ncomp, theta_pix, kinds=("lens", "delens")):
+        """Create the lens slots of one shape and capture the graphs of every batch bucket now, before
+        ``start``.  Otherwise the scheduler thread does it the first time a shape or bucket arrives: pinned
+        host and device buffers (about 3 GB per slot for 1024^2 QU at max_batch 16) and a capture, during
+        which every queued lens batch waits."""
+        if self._thread.is_alive():
+            raise RuntimeError("Server.prepare must be called before start()")
+        torch.cuda.set_device(self.dev)
+        for kind in kinds:
+            key = (int(nside), int(ncomp), float(theta_pix), nat_direction(kind))
+            ss = self.slots.setdefault(key, [])
+            while len(ss) < 2:
+                N, C, th, direction = key
+                ss.append(_LensSlot(self.dev, N, C, th, direction, self.max_batch, 7, self.use_graphs,
+                                    self.lens_priority))
+            if self.use_graphs:
+                for s in ss:
+                    bb = 1
+                    while True:
+                        s._graph(min(bb, s.cap))
+                        if bb >= s.cap:
+                            break
+                        bb *= 2
+        torch.cuda.synchronize(self.dev)
+        return self
 
     # ---------------------------------------------------------- internal
     def _release(self, nbytes):

@@ -96,3 +96,27 @@ def test_tight_budget_still_completes_and_singular_phi_fails_alone(torch_cuda):
     srv.stop()
     assert all(r.error is None for r in good)
     assert isinstance(bad.error, nat.SingularMagnificationError)
+
+
+def test_prepared_slots_serve_without_new_captures(torch_cuda):
+    """Server.prepare creates a shape's slots and every bucket's graph up front; serving then adds none."""
+    from cmblensing_b200.serve import Server, run_alone
+    srv = Server(max_batch=4, wf_workers=1).prepare(128, 2, 3.0)
+    keys = sorted(srv.slots)
+    assert [k[3] for k in keys] == [-1, 1] and all(len(srv.slots[k]) == 2 for k in keys)
+    graphs = {k: [sorted(s.graphs) for s in srv.slots[k]] for k in keys}
+    assert all(g == [1, 2, 4] for gs in graphs.values() for g in gs)
+    reqs = [_lens_req(["lens", "delens"][i % 2], 128, 2, 3.0, seed=50 + i) for i in range(7)]
+    srv.start()
+    with pytest.raises(RuntimeError):
+        srv.prepare(128, 1, 3.0)
+    for r in reqs:
+        srv.submit(r)
+    for r in reqs:
+        assert r.done.wait(120)
+    srv.stop()
+    assert sorted(srv.slots) == keys
+    assert {k: [sorted(s.graphs) for s in srv.slots[k]] for k in keys} == graphs
+    for r in reqs:
+        assert r.error is None, r.error
+        assert np.array_equal(r.result, run_alone(r))
