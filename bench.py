@@ -291,10 +291,11 @@ def p_plane_bytes_per_lens(n, P):
 
 
 def phi_pp_bytes_per_map(n, P):
-    """The phi precompute with the p planes formed in its row pass (lf_phi_precompute_pp), per map:
-    row r2c (read phi 8, write the half spectrum 8), in-place column FFT (8 + 8), derivative columns
-    (read 8, write five packed spectra 40), fused row pass (read 40, write p at 2n+1 times 8 (2n+1))."""
-    return (16 + 16 + 48 + 40 + 8 * (2 * n + 1)) * P
+    """The phi precompute with the p planes formed in its row pass (lf_phi_precompute_pp, no derivative
+    planes requested), per map: row r2c (read phi 8, write the half spectrum 8), in-place column FFT
+    (8 + 8), derivative columns (read 8, write five packed float32 spectra 20), fused row pass (read 20,
+    write p at 2n+1 times 8 (2n+1))."""
+    return (16 + 16 + 28 + 20 + 8 * (2 * n + 1)) * P
 
 
 def survey_bytes_per_map(C, n, P):

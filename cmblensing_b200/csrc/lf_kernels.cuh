@@ -984,9 +984,10 @@ __global__ void __launch_bounds__(NT) k_phi_cols_fwd(double2* __restrict__ arr, 
 //   G2 = IFFT_col(-KX^2 F):     phi_xx = G2
 // (the 1/N^2 of irfft2 folded into the column multiplier).  ``spec`` is the
 // unpacked rfft2 of phi; ``packed`` is [B][5][N][N/2] complex.
-template <int N, int LINES, int NT>
-__global__ void __launch_bounds__(NT) k_phi_cols_deriv(const double2* __restrict__ spec, double2* __restrict__ packed,
+template <int N, int LINES, int NT, typename PK = double2>
+__global__ void __launch_bounds__(NT) k_phi_cols_deriv(const double2* __restrict__ spec, PK* __restrict__ packed,
                                                         const double2* __restrict__ twN, double kbase) {
+  using S = decltype(PK::x);  // storage precision of the packed derivative spectra
   constexpr int H = N / 2;
   extern __shared__ __align__(16) unsigned char smem_raw[];
   double2* tw = reinterpret_cast<double2*>(smem_raw);
@@ -1020,7 +1021,7 @@ __global__ void __launch_bounds__(NT) k_phi_cols_deriv(const double2* __restrict
     for (int o = 0; o < 2; ++o) {
       const int j = kOut[g][o][0], pw = kOut[g][o][1];
       if (j < 0) continue;
-      double2* out = packed + (map * 5 + j) * (long)N * H;
+      PK* out = packed + (map * 5 + j) * (long)N * H;
       for (int idx = tid; idx < N * LINES; idx += NT) {
         const int m = idx / LINES, line = idx % LINES;
         const int col = c0 + line;
@@ -1031,9 +1032,9 @@ __global__ void __launch_bounds__(NT) k_phi_cols_deriv(const double2* __restrict
         if (pw == 0) v = G;
         else if (pw == 1) v = make_double2(-ky * G.y, ky * G.x);
         else v = make_double2(-ky * ky * G.x, -ky * ky * G.y);
-        if (col == 0) reinterpret_cast<double*>(out + (long)m * H)[0] = v.x;
-        else if (col == H) reinterpret_cast<double*>(out + (long)m * H)[1] = v.x;
-        else out[(long)m * H + col] = v;
+        if (col == 0) reinterpret_cast<S*>(out + (long)m * H)[0] = S(v.x);
+        else if (col == H) reinterpret_cast<S*>(out + (long)m * H)[1] = S(v.x);
+        else out[(long)m * H + col] = PK{S(v.x), S(v.y)};
       }
     }
     __syncthreads();
@@ -1106,8 +1107,8 @@ __global__ void k_min_det(const T* __restrict__ planes, long P, int* __restrict_
 // 64-map 512^2 step).
 __host__ __device__ constexpr int pp_threads(int n) { return n <= 64 ? 64 : (n == 128 ? 96 : (n <= 512 ? 160 : 320)); }
 
-template <int N, int LINES, int NT>
-__global__ void __launch_bounds__(NT, N == 1024 ? 2 : 4) k_phi_rows_c2r_pp(const double2* __restrict__ packed, float* __restrict__ planes,
+template <int N, int LINES, int NT, typename PK = double2>
+__global__ void __launch_bounds__(NT, N == 1024 ? 2 : 4) k_phi_rows_c2r_pp(const PK* __restrict__ packed, float* __restrict__ planes,
                                                          float* __restrict__ pp, int K, int* __restrict__ min_det,
                                                          const double2* __restrict__ twN) {
   constexpr int H = N / 2;
@@ -1124,7 +1125,7 @@ __global__ void __launch_bounds__(NT, N == 1024 ? 2 : 4) k_phi_rows_c2r_pp(const
   table_copy<N>(tw, twN, mbar, tid);
 #pragma unroll
   for (int j = 0; j < 5; ++j)
-    load_rows<double, double2, H, LINES, NT>(buf + j * TILE, packed + ((map * 5 + j) * N + r0) * (long)H, H, tid);
+    load_rows<double, PK, H, LINES, NT>(buf + j * TILE, packed + ((map * 5 + j) * N + r0) * (long)H, H, tid);
   __syncthreads();
   table_wait(mbar);
   c2r_pre<double, H, LINES, 5, NT>(buf, tw, tid);

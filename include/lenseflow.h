@@ -93,7 +93,10 @@ float lf_decode_min_det(int encoded);
  * k / (2n), k = 0..2n, ascending: [batch][2n+1][2][N][N] (lf_pp_bytes).  One
  * set serves the forward, inverse and adjoint lens with n steps.  ``planes``
  * (optional, NULL to skip) receives the five derivative planes as
- * lf_phi_precompute writes them; ``min_det`` as in lf_phi_precompute.
+ * lf_phi_precompute writes them; ``min_det`` as in lf_phi_precompute.  Every
+ * transform is float64; without ``planes`` the derivative spectra between the
+ * column and row transforms are stored as float32 (the p planes differ from
+ * those of the planes-requested call by float32 rounding, about 1e-7). 
  * Workspace: lf_phi_workspace_bytes.  Replaces get_primal_derivatives
  * (util.py:110-130) plus the per-RHS p computation of the reference. */
 size_t lf_pp_bytes(lf_plan_t plan, int batch, int nsteps);

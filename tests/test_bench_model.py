@@ -37,10 +37,11 @@ def test_column_and_p_plane_bytes():
 
 
 def test_fused_phi_precompute_saves_the_plane_round_trip():
-    # the derivative planes (20 N^2 written, 20 N^2 read back) no longer cross HBM on the p-plane path
+    # the derivative planes (20 N^2 written, 20 N^2 read back) no longer cross HBM on the p-plane path, and
+    # the five derivative spectra cross it as float32 (20 N^2 written and read instead of 40)
     n = 7
-    assert bench.phi_pp_bytes_per_map(n, P) == (120 + 8 * 15) * P
-    assert 140 * P + bench.p_plane_bytes_per_lens(n, P) - bench.phi_pp_bytes_per_map(n, P) == 40 * P
+    assert bench.phi_pp_bytes_per_map(n, P) == (80 + 8 * 15) * P
+    assert 140 * P + bench.p_plane_bytes_per_lens(n, P) - bench.phi_pp_bytes_per_map(n, P) == 80 * P
 
 
 def test_stage1_bytes_match_the_stage_model():
