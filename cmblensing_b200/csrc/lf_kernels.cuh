@@ -21,6 +21,7 @@
 
 #include "lf_fft.cuh"
 
+
 namespace lf {
 
 // ----------------------------------------------------------- parameters
@@ -499,6 +500,10 @@ template <int LINES>
 constexpr size_t row_pair_smem_bytes(int n) {
   return sizeof(float2) * (n + 2 * LINES * n) + sizeof(float) * 6 * LINES * n + 16;
 }
+template <int LINES>
+constexpr size_t row_pair_fwd_smem_bytes(int n) {  // k_row_pair: p_x, p_y in registers, four staged planes
+  return sizeof(float2) * (n + 2 * LINES * n) + sizeof(float) * 4 * LINES * n + 16;
+}
 
 template <int N, int LINES, int NT, int MINB>
 __global__ void __launch_bounds__(NT, MINB) k_row_pair(StageArgs a) {
@@ -515,8 +520,8 @@ __global__ void __launch_bounds__(NT, MINB) k_row_pair(StageArgs a) {
   extern __shared__ __align__(16) unsigned char smem_raw[];
   c2<T>* tw = reinterpret_cast<c2<T>*>(smem_raw);
   c2<T>* buf = tw + N;                                 // tile c at buf + c * TILE
-  T* stg = reinterpret_cast<T*>(buf + 2 * TILE);       // y0_0, y0_1, acc_0, acc_1, p_x, p_y
-  uint64_t* mbar = reinterpret_cast<uint64_t*>(stg + 6 * RB);  // [0]: staged update operands, [1]: spectra
+  T* stg = reinterpret_cast<T*>(buf + 2 * TILE);       // y0_0, y0_1, acc_0, acc_1
+  uint64_t* mbar = reinterpret_cast<uint64_t*>(stg + 4 * RB);  // [0]: staged update operands, [1]: spectra
   const int tid = threadIdx.x;
   const int r0 = blockIdx.x * LINES;
   const long map = blockIdx.y;
@@ -540,17 +545,28 @@ __global__ void __launch_bounds__(NT, MINB) k_row_pair(StageArgs a) {
       bulk_g2s(buf + c * TILE, spec(a.gx, c), LINES * H * sizeof(c2<T>), mbar + 1);
       bulk_g2s(buf + c * TILE + LINES * H, spec(a.s, c), LINES * H * sizeof(c2<T>), mbar + 1);
     }
-    mbar_expect_tx(mbar, uint32_t((with_acc ? 6 : 4) * RB * sizeof(T)));
-    const T* pp = reinterpret_cast<const T*>(a.pp) + (map * a.pp_k + a.pp_idx) * 2 * P + prow0;
+    mbar_expect_tx(mbar, uint32_t((with_acc ? 4 : 2) * RB * sizeof(T)));
     for (int c = 0; c < 2; ++c) {
       bulk_g2s(stg + c * RB, reinterpret_cast<const T*>(a.y0) + (map * 2 + c) * P + prow0, RB * sizeof(T), mbar);
       if (with_acc)
         bulk_g2s(stg + (2 + c) * RB, reinterpret_cast<const T*>(a.acc) + (map * 2 + c) * P + prow0, RB * sizeof(T),
                  mbar);
-      bulk_g2s(stg + (4 + c) * RB, pp + c * P, RB * sizeof(T), mbar);
     }
   }
   pdl_wait();  // every thread, before its own global reads and writes
+  // p_x, p_y of the thread's 8 update pixels straight into registers (coalesced; their latency hides under
+  // the transforms): without their staging a block needs 36.9 instead of 45.1 KB of shared memory, so six
+  // blocks fit on an SM instead of five (row passes 4.51-4.53 -> 4.48-4.49 ms per 64-map step)
+  T preg[2][R];
+  {
+    const T* pq = reinterpret_cast<const T*>(a.pp) + (map * a.pp_k + a.pp_idx) * 2 * P + prow0 + (tid / NB) * N +
+                  tid % NB;
+#pragma unroll
+    for (int r = 0; r < R; ++r) {
+      preg[0][r] = __ldg(pq + NB * r);
+      preg[1][r] = __ldg(pq + P + NB * r);
+    }
+  }
   constexpr int O8 = ptw_offset(N, R, R), O64 = ptw_offset(N, R, R * R);
   const T ky_scale = T(a.kbase / double(N));
   __syncthreads();  // barriers initialised before anyone waits on them
@@ -619,13 +635,11 @@ __global__ void __launch_bounds__(NT, MINB) k_row_pair(StageArgs a) {
   const long prow = prow0 + (long)row * N;
   const T* sy0 = stg + row * N;
   const T* sacc = stg + 2 * RB + row * N;
-  const T* spx = stg + 4 * RB + row * N;
-  const T* spy = stg + 5 * RB + row * N;
   const T hh = T(a.h);
 #pragma unroll
   for (int r = 0; r < R; ++r) {
     const int n = j + NB * r;
-    const T px = spx[n], py = spy[n];
+    const T px = preg[0][r], py = preg[1][r];
 #pragma unroll
     for (int c = 0; c < 2; ++c) {
       const T k = px * v[c][r].x + py * v[c][r].y;
