@@ -275,7 +275,7 @@ def col_bytes_per_lens(C, n, P):
 # launch are stage1_bytes_per_map(C) N^2; the reads equal them, the writes
 # fall short by what is still in L2 when the launch ends.
 NCU_STAGE1_TRAFFIC_PER_MAP = {
-    ("k_row_pair", 512, 2): (268.48e6 + 97.70e6) / 32,
+    ("k_row_pair", 512, 2): (268.50e6 + 96.53e6) / 32,
     ("k_row_pair_adj", 512, 2): (134.27e6 + 51.79e6) / 16,
 }
 

@@ -310,14 +310,14 @@ cudaError_t run_lens_pp(const StageArgs& base, int B, int nsteps, double t0, dou
         // 2-row tiles, 128 threads (measured best of 1, 2 and 4 rows: 6.81, 5.48 and
         // 5.96 ms of row passes per 64-map step), six blocks per SM
         constexpr int PL = 2, PNT = (N / 8) * PL;
-        e = launch_k<k_row_pair<N, PL, PNT, 6>>(LF_KIND_ROW, dim3(N / PL, B), PNT, row_pair_fwd_smem_bytes<PL>(N),
+        e = launch_k<k_row_pair<N, PL, PNT, 6>>(LF_KIND_ROW, dim3(N / PL, B), PNT, row_pair_smem_bytes<PL>(N),
                                                 st, a);
       } else if constexpr (PP && C == 2 && ADJ && N == 512 && std::is_same<T, float>::value) {
         // adjoint counterpart: one inverse transform for both rates, two forward
         // transforms (p_x y, p_y y) for the next stage; same tile shape
         constexpr int PL = 2, PNT = (N / 8) * PL;
-        e = launch_k<k_row_pair_adj<N, PL, PNT, 4>>(LF_KIND_ROW, dim3(N / PL, B), PNT, row_pair_smem_bytes<PL>(N),
-                                                    st, a);
+        e = launch_k<k_row_pair_adj<N, PL, PNT, 6>>(LF_KIND_ROW, dim3(N / PL, B), PNT,
+                                                    row_pair_smem_bytes<PL>(N), st, a);
       } else {
         e = launch_k<k_row<T, N, C, ADJ, false, RL, RNT, false, RMB, PP>>(LF_KIND_ROW, grow, RNT, smem_row, st, a);
       }

@@ -493,15 +493,12 @@ __global__ void __launch_bounds__(NT, MINB) k_row(StageArgs a) {
 // 16-byte global load and store phases, and the inverse transform's last
 // radix-8 pass, the pointwise update and the forward transform's first pass
 // run in registers: both passes see x[j + 64 r] of one row in one thread.
-// The update's operands (y0, acc, p_x, p_y of the tile's rows: contiguous
-// blocks) are fetched into shared memory by bulk copies issued at the start,
-// so their latency overlaps the loads and the first inverse passes.
+// The update's operands y0 and acc (the tile's rows: contiguous blocks) are
+// fetched into shared memory by bulk copies issued at the start, and each
+// thread loads its pixels' p_x, p_y into registers, so their latency overlaps
+// the loads and the first inverse passes.
 template <int LINES>
-constexpr size_t row_pair_smem_bytes(int n) {
-  return sizeof(float2) * (n + 2 * LINES * n) + sizeof(float) * 6 * LINES * n + 16;
-}
-template <int LINES>
-constexpr size_t row_pair_fwd_smem_bytes(int n) {  // k_row_pair: p_x, p_y in registers, four staged planes
+constexpr size_t row_pair_smem_bytes(int n) {  // paired row passes: p_x, p_y in registers, four staged planes
   return sizeof(float2) * (n + 2 * LINES * n) + sizeof(float) * 4 * LINES * n + 16;
 }
 
@@ -726,8 +723,8 @@ __global__ void __launch_bounds__(NT, MINB) k_row_pair_adj(StageArgs a) {
   extern __shared__ __align__(16) unsigned char smem_raw[];
   c2<T>* tw = reinterpret_cast<c2<T>*>(smem_raw);
   c2<T>* buf = tw + N;                            // Z (tile 0); then w_u (tile 0), w_v (tile 1)
-  T* stg = reinterpret_cast<T*>(buf + 2 * TILE);  // y0_0, y0_1, acc_0, acc_1, p_x, p_y
-  uint64_t* mbar = reinterpret_cast<uint64_t*>(stg + 6 * RB);  // [0]: staged update operands, [1]: spectra
+  T* stg = reinterpret_cast<T*>(buf + 2 * TILE);  // y0_0, y0_1, acc_0, acc_1
+  uint64_t* mbar = reinterpret_cast<uint64_t*>(stg + 4 * RB);  // [0]: staged update operands, [1]: spectra
   const int tid = threadIdx.x;
   const int r0 = blockIdx.x * LINES;
   const long map = blockIdx.y;
@@ -751,17 +748,26 @@ __global__ void __launch_bounds__(NT, MINB) k_row_pair_adj(StageArgs a) {
       bulk_g2s(buf + c * TILE, spec(a.gx, c), LINES * H * sizeof(c2<T>), mbar + 1);
       bulk_g2s(buf + c * TILE + LINES * H, spec(a.v, c), LINES * H * sizeof(c2<T>), mbar + 1);
     }
-    mbar_expect_tx(mbar, uint32_t((with_acc ? 6 : 4) * RB * sizeof(T)));
-    const T* pp = reinterpret_cast<const T*>(a.pp) + (map * a.pp_k + a.pp_idx) * 2 * P + prow0;
+    mbar_expect_tx(mbar, uint32_t((with_acc ? 4 : 2) * RB * sizeof(T)));
     for (int c = 0; c < 2; ++c) {
       bulk_g2s(stg + c * RB, reinterpret_cast<const T*>(a.y0) + (map * 2 + c) * P + prow0, RB * sizeof(T), mbar);
       if (with_acc)
         bulk_g2s(stg + (2 + c) * RB, reinterpret_cast<const T*>(a.acc) + (map * 2 + c) * P + prow0, RB * sizeof(T),
                  mbar);
-      bulk_g2s(stg + (4 + c) * RB, pp + c * P, RB * sizeof(T), mbar);
     }
   }
   pdl_wait();  // every thread, before its own global reads and writes
+  // p_x, p_y (next stage's time) of the thread's 8 update pixels in registers, as in k_row_pair: six blocks fit
+  T preg[2][R];
+  {
+    const T* pq = reinterpret_cast<const T*>(a.pp) + (map * a.pp_k + a.pp_idx) * 2 * P + prow0 + (tid / NB) * N +
+                  tid % NB;
+#pragma unroll
+    for (int r = 0; r < R; ++r) {
+      preg[0][r] = __ldg(pq + NB * r);
+      preg[1][r] = __ldg(pq + P + NB * r);
+    }
+  }
   constexpr int O8 = ptw_offset(N, R, R), O64 = ptw_offset(N, R, R * R);
   const T ky_scale = T(a.kbase / double(N));
   __syncthreads();  // barriers initialised before anyone waits on them
@@ -818,8 +824,6 @@ __global__ void __launch_bounds__(NT, MINB) k_row_pair_adj(StageArgs a) {
   const long prow = prow0 + (long)row * N;
   const T* sy0 = stg + row * N;
   const T* sacc = stg + 2 * RB + row * N;
-  const T* spx = stg + 4 * RB + row * N;
-  const T* spy = stg + 5 * RB + row * N;
   const T hh = T(a.h);
   c2<T> wu[R], wv[R];
 #pragma unroll
@@ -848,7 +852,7 @@ __global__ void __launch_bounds__(NT, MINB) k_row_pair_adj(StageArgs a) {
         }
       }
     }
-    const T px = spx[n], py = spy[n];  // p at the next stage's time
+    const T px = preg[0][r], py = preg[1][r];  // p at the next stage's time
     wu[r] = mk<T>(px * yn[0], px * yn[1]);
     wv[r] = mk<T>(py * yn[0], py * yn[1]);
   }
