@@ -269,14 +269,13 @@ def col_bytes_per_lens(C, n, P):
 
 # DRAM bytes (dram__bytes_read.sum + dram__bytes_write.sum) per map of one RK4
 # stage-1 launch of the dominant row kernel, from one ncu capture each: the
-# forward kernel's 21st launch in a 32-map step (RK4 step 6, stage 1), the
-# adjoint kernel's 13th in a 16-map step (step 4, stage 1); the capture's
+# 21st launch of each kernel in a 32-map step (RK4 step 6, stage 1); the capture's
 # traffic scales with the maps of the launch.  The algorithmic bytes of that
 # launch are stage1_bytes_per_map(C) N^2; the reads equal them, the writes
 # fall short by what is still in L2 when the launch ends.
 NCU_STAGE1_TRAFFIC_PER_MAP = {
     ("k_row_pair", 512, 2): (268.50e6 + 96.53e6) / 32,
-    ("k_row_pair_adj", 512, 2): (134.27e6 + 51.79e6) / 16,
+    ("k_row_pair_adj", 512, 2): (268.49e6 + 151.81e6) / 32,
 }
 
 
@@ -669,7 +668,7 @@ def main():
               "vs_baseline": None, "dtype": "f32", "data": "synthetic", "config": workload_config(a),
               "roofline": {"bound": "hbm", "kernel": kname, "achieved": achieved, "peak": hbm_peak,
                            "unit": "GB/s", "frac": achieved / hbm_peak, "traffic": traffic,
-                           "traffic_launch": "RK4 stage 1 (ncu capture of a 32-map forward / 16-map adjoint step, scaled to the batch)"
+                           "traffic_launch": "RK4 stage 1 (ncu capture of a 32-map step, scaled to the batch)"
                            if traffic is not None else None,
                            "traffic_launch_algorithmic_bytes": stage1_bytes_per_map(C, a.adjoint) * P * B
                            if traffic is not None else None,
