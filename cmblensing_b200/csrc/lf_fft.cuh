@@ -31,6 +31,7 @@
 
 #include <type_traits>
 
+
 namespace lf {
 
 // Pure-arithmetic helpers and the register DFTs compile for the host as well
@@ -43,8 +44,48 @@ template <> struct V2<double> { using type = double2; };
 template <typename T> using c2 = typename V2<T>::type;
 
 template <typename T> LF_HD c2<T> mk(T x, T y) { c2<T> r; r.x = x; r.y = y; return r; }
-template <typename T> LF_HD c2<T> cadd(c2<T> a, c2<T> b) { return mk<T>(a.x + b.x, a.y + b.y); }
-template <typename T> LF_HD c2<T> csub(c2<T> a, c2<T> b) { return mk<T>(a.x - b.x, a.y - b.y); }
+// sm_100 packed float32 pairs (add/sub/fma.rn.f32x2): one instruction per complex
+// add, subtract or a + s u with a real s, where scalar code needs two.  Device
+// float code only; the host build (the DFT unit test) keeps the scalar form.
+// Measured on the two-pass column pass (64-map 512^2 QU step): add/sub 1.81 ->
+// 1.63 ms, with the butterflies' a +- s u as well 1.56 ms.
+__device__ __forceinline__ float2 f2_add(float2 a, float2 b) {
+  uint64_t r;
+  asm("add.rn.f32x2 %0, %1, %2;" : "=l"(r) : "l"(*reinterpret_cast<uint64_t*>(&a)), "l"(*reinterpret_cast<uint64_t*>(&b)));
+  return *reinterpret_cast<float2*>(&r);
+}
+__device__ __forceinline__ float2 f2_sub(float2 a, float2 b) {
+  uint64_t r;
+  asm("sub.rn.f32x2 %0, %1, %2;" : "=l"(r) : "l"(*reinterpret_cast<uint64_t*>(&a)), "l"(*reinterpret_cast<uint64_t*>(&b)));
+  return *reinterpret_cast<float2*>(&r);
+}
+template <typename T> LF_HD c2<T> cadd(c2<T> a, c2<T> b) {
+#ifdef __CUDA_ARCH__
+  if constexpr (std::is_same<T, float>::value) return f2_add(a, b);
+#endif
+  return mk<T>(a.x + b.x, a.y + b.y);
+}
+template <typename T> LF_HD c2<T> csub(c2<T> a, c2<T> b) {
+#ifdef __CUDA_ARCH__
+  if constexpr (std::is_same<T, float>::value) return f2_sub(a, b);
+#endif
+  return mk<T>(a.x - b.x, a.y - b.y);
+}
+__device__ __forceinline__ float2 f2_fma(float2 a, float2 b, float2 c) {
+  uint64_t r;
+  asm("fma.rn.f32x2 %0, %1, %2, %3;"
+      : "=l"(r)
+      : "l"(*reinterpret_cast<uint64_t*>(&a)), "l"(*reinterpret_cast<uint64_t*>(&b)),
+        "l"(*reinterpret_cast<uint64_t*>(&c)));
+  return *reinterpret_cast<float2*>(&r);
+}
+// a + s u for a real s
+template <typename T> LF_HD c2<T> caxpy(T s, c2<T> u, c2<T> a) {
+#ifdef __CUDA_ARCH__
+  if constexpr (std::is_same<T, float>::value) return f2_fma(make_float2(s, s), u, a);
+#endif
+  return mk<T>(a.x + s * u.x, a.y + s * u.y);
+}
 template <typename T> LF_HD c2<T> cmul(c2<T> a, c2<T> b) {
   return mk<T>(a.x * b.x - a.y * b.y, a.x * b.y + a.y * b.x);
 }
@@ -95,21 +136,19 @@ template <typename T, bool INV> LF_HD void dft8(c2<T>* a) {
   dft4<T, INV>(e);
   dft4<T, INV>(o);
   const T c = T(LF_C45);
-  // o1 * W8^1, W8^1 = (c, -c) forward / (c, c) inverse
-  c2<T> o1 = INV ? mk<T>(c * (o[1].x - o[1].y), c * (o[1].x + o[1].y))
-                 : mk<T>(c * (o[1].x + o[1].y), c * (o[1].y - o[1].x));
+  // o1 * W8^1 = c s1, W8^1 = (c, -c) forward / (c, c) inverse
+  const c2<T> s1 = INV ? mk<T>(o[1].x - o[1].y, o[1].x + o[1].y) : mk<T>(o[1].x + o[1].y, o[1].y - o[1].x);
   c2<T> o2 = rot90<T, INV>(o[2]);
-  // o3 * W8^3, W8^3 = (-c, -c) forward / (-c, c) inverse
-  c2<T> o3 = INV ? mk<T>(-c * (o[3].x + o[3].y), c * (o[3].x - o[3].y))
-                 : mk<T>(c * (o[3].y - o[3].x), -c * (o[3].x + o[3].y));
+  // o3 * W8^3 = c s3, W8^3 = (-c, -c) forward / (-c, c) inverse
+  const c2<T> s3 = INV ? mk<T>(-o[3].x - o[3].y, o[3].x - o[3].y) : mk<T>(o[3].y - o[3].x, -o[3].x - o[3].y);
   a[0] = cadd<T>(e[0], o[0]);
   a[4] = csub<T>(e[0], o[0]);
-  a[1] = cadd<T>(e[1], o1);
-  a[5] = csub<T>(e[1], o1);
+  a[1] = caxpy<T>(c, s1, e[1]);
+  a[5] = caxpy<T>(-c, s1, e[1]);
   a[2] = cadd<T>(e[2], o2);
   a[6] = csub<T>(e[2], o2);
-  a[3] = cadd<T>(e[3], o3);
-  a[7] = csub<T>(e[3], o3);
+  a[3] = caxpy<T>(c, s3, e[3]);
+  a[7] = caxpy<T>(-c, s3, e[3]);
 }
 
 // a <- a + w b, b <- a - w b for a constant twiddle w = (wr, wi), with FMAs: w b is written as
@@ -128,8 +167,8 @@ template <typename T> LF_HD void bfly_w(c2<T>& a, c2<T>& b, double wr, double wi
     f = T(wi);
   }
   const c2<T> a0 = a;
-  a = mk<T>(a0.x + f * u.x, a0.y + f * u.y);
-  b = mk<T>(a0.x - f * u.x, a0.y - f * u.y);
+  a = caxpy<T>(f, u, a0);
+  b = caxpy<T>(-f, u, a0);
 }
 
 // Radix-2 split into two 8-point DFTs: X[k] = E[k] + W16^k O[k], X[k+8] = E[k] - W16^k O[k].
