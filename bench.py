@@ -467,7 +467,7 @@ def _serve_stream(srv, make, rng, rate, nreq, warm=0):
 
 
 def _serve_summary(reqs, span, ok):
-    from cmblensing_b200.serve import latency_summary
+    from cmblensing_b200.serve import latency_summary, lens_tail_breakdown
     wsum = sum(r.nside * r.nside * r.ncomp for r in reqs if r.error is None) / (512.0 * 512.0 * 2)
     lat = [r for r in reqs if r.latency is not None]
     k = max(1, len(lat) // 10)
@@ -479,6 +479,7 @@ def _serve_summary(reqs, span, ok):
             "latency": latency_summary(reqs),
             "latency_by_kind": {kd: latency_summary([r for r in reqs if r.kind == kd])
                                 for kd in ("lens", "delens", "wf")},
+            "lens_tail_1pct": lens_tail_breakdown(reqs),
             # a bounded queue: the last tenth of the stream waits no longer than the first
             "p50_first_tenth_ms": latency_summary(lat[:k]).get("p50_ms"),
             "p50_last_tenth_ms": latency_summary(lat[-k:]).get("p50_ms")}

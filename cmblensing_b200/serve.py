@@ -23,6 +23,7 @@ from __future__ import annotations
 
 import collections
 import queue
+import sys
 import threading
 import time
 
@@ -57,6 +58,9 @@ class Request:
         self.wf_kwargs = wf_kwargs or {}
         self.t_submit = None
         self.t_done = None
+        # lens / delens stages (host clock): admitted by the scheduler, batch launch begun, launch issued
+        # (inputs staged, graph replayed), completion seen by the scheduler's poll
+        self.t_admit = self.t_launch = self.t_issued = self.t_seen = None
         self.result = None
         self.error = None
         self.done = threading.Event()
@@ -136,6 +140,9 @@ class _LensSlot:
         b = len(reqs)
         self.reqs = reqs
         self.busy = True
+        t0 = time.perf_counter()
+        for r in reqs:
+            r.t_launch = t0
         for i, r in enumerate(reqs):
             # torch converts float64 -> float32 inside the copy, multi-threaded and without the GIL
             self.h_f[i].copy_(torch.from_numpy(np.ascontiguousarray(r.f)))
@@ -153,6 +160,9 @@ class _LensSlot:
             self.h_md[:b].copy_(self.md[:b], non_blocking=True)
             self.event = torch.cuda.Event()
             self.event.record(self.stream)
+        t1 = time.perf_counter()
+        for r in reqs:
+            r.t_issued = t1
 
     def poll(self):
         """Complete the batch's requests if its event has fired; return them."""
@@ -172,7 +182,7 @@ class _LensSlot:
                 r.error = nat.SingularMagnificationError(nat.LF_ERR_SINGULAR_MAGNIFICATION, f"min det {md:.3g}")
             else:
                 r.result = out[i]
-            r.t_done = now
+            r.t_seen = r.t_done = now
             r.done.set()
         self.busy = False
         self.reqs = []
@@ -183,7 +193,7 @@ class Server:
     """Continuous-batching scheduler over the LenseFlow engine on one GPU."""
 
     def __init__(self, hbm_budget=32 << 30, max_batch=16, use_graphs=True, wf_workers=2, wf_batch=8, device=None,
-                 lens_priority=-1):
+                 lens_priority=-1, gil_switch_s=5e-4):
         self.dev = torch.device("cuda", torch.cuda.current_device() if device is None else torch.device(device).index)
         self.budget = int(hbm_budget)
         self.max_batch = int(max_batch)
@@ -193,6 +203,7 @@ class Server:
         # mixed stream: 41 maps/s, lens p99 ~0.5 s, WF p50 ~4 s, against 33 maps/s, 1.2 s and 5.1 s
         # with four workers at equal priority.
         self.lens_priority = int(lens_priority)
+        self.gil_switch_s = gil_switch_s  # interpreter switch interval while serving (None: leave it)
         self.inbox = queue.Queue()
         self.pending = collections.defaultdict(collections.deque)  # group key -> requests
         self.slots = {}  # group key -> list of _LensSlot
@@ -209,6 +220,13 @@ class Server:
 
     # ------------------------------------------------------------ client
     def start(self):
+        # The scheduler thread makes a few dozen short GIL-releasing calls per batch (copies, graph replays,
+        # event queries) while the Wiener-filter workers keep the interpreter busy; each call must win the
+        # GIL back, which under contention takes up to the switch interval.  A shorter interval while the
+        # server runs bounds that wait (restored by stop()).
+        self._switch = sys.getswitchinterval()
+        if self.gil_switch_s is not None:
+            sys.setswitchinterval(min(self._switch, self.gil_switch_s))
         self._thread.start()
         for t in self._wf_threads:
             t.start()
@@ -227,6 +245,8 @@ class Server:
             self.wf_cond.notify_all()
         for t in self._wf_threads:
             t.join()
+        if getattr(self, "_switch", None) is not None:
+            sys.setswitchinterval(self._switch)
 
     def prepare(self, nside, ncomp, theta_pix, kinds=("lens", "delens")):
         """Create the lens slots of one shape and capture the graphs of every batch bucket now, before
@@ -300,6 +320,7 @@ class Server:
             # 3. admit by footprint, in arrival order
             while waiting and self._admit(waiting[0].footprint()):
                 r = waiting.popleft()
+                r.t_admit = time.perf_counter()
                 if r.kind == "wf":
                     with self.wf_cond:
                         self.wf_pending[(r.nside, r.ncomp, r.theta_pix)].append(r)
@@ -396,6 +417,23 @@ def run_alone(req):
     phi = torch.as_tensor(np.asarray(req.phi, dtype=np.float64), device="cuda").unsqueeze(0)
     pp = plan.phi_pp(phi, req.n, check_det=True)
     return plan.lense_flow_pp(f, pp, req.n, direction=nat_direction(req.kind))[0].cpu().numpy()
+
+
+def lens_tail_breakdown(reqs, frac=0.01):
+    """For the slowest ``frac`` of the completed lens / delens requests: mean ms spent waiting for admission,
+    queued for a slot (admitted -> launch begun), staging and issuing the batch, and on the GPU until the
+    scheduler saw the batch complete."""
+    done = [r for r in reqs if r.kind in ("lens", "delens") and r.t_seen is not None and r.t_launch is not None]
+    if not done:
+        return {}
+    done.sort(key=lambda r: r.latency)
+    tail = done[-max(1, int(round(frac * len(done)))):]
+    ms = lambda f: float(np.mean([f(r) for r in tail]) * 1e3)
+    return {"n": len(tail), "latency_ms": ms(lambda r: r.latency),
+            "admission_ms": ms(lambda r: r.t_admit - r.t_submit),
+            "slot_wait_ms": ms(lambda r: r.t_launch - r.t_admit),
+            "stage_and_issue_ms": ms(lambda r: r.t_issued - r.t_launch),
+            "gpu_until_seen_ms": ms(lambda r: r.t_seen - r.t_issued)}
 
 
 def latency_summary(reqs):
