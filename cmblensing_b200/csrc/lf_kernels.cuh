@@ -21,8 +21,6 @@
 
 #include "lf_fft.cuh"
 
-
-
 namespace lf {
 
 // ----------------------------------------------------------- parameters
