@@ -63,3 +63,16 @@ def test_workload_names():
     A.adjoint = True
     assert bench.workload_config(A)["workload"] == "lenseflow_adj_qu512_b64_n7"
     assert bench.metric_name(A) == bench.METRIC_ADJ
+
+
+def test_per_map_totals_for_the_headline_workload():
+    # 512^2 QU, n = 7, new phi per map: the totals the design notes quote (MB = 1e6 bytes)
+    n, C = 7, 2
+    rows = bench.row_bytes_per_lens(C, n, P)
+    cols = bench.col_bytes_per_lens(C, n, P)
+    phi = bench.phi_pp_bytes_per_map(n, P)
+    assert round(rows / 1e6, 1) == 400.6
+    assert round(cols / 1e6, 1) == 117.4
+    assert round(phi / 1e6, 1) == 52.4
+    assert round((rows + cols + phi) / 1e6, 1) == 570.4
+    assert round(bench.survey_bytes_per_map(C, n, P) / 1e6, 1) == 716.2
